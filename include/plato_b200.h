@@ -1,0 +1,248 @@
+/*
+ * plato_b200.h — C ABI of the B200-native dual-mode push/pull graph engine.
+ *
+ * Plain C types only (no torch, no C++): every entry point returns an int
+ * status (PLATO_OK == 0) and never aborts; the message of the last failure on
+ * the calling thread is available from plato_last_error().
+ *
+ * Vertex ids are the caller's ids, which must be compact (every id in
+ * [0, vertices) — the reference requires the same, see
+ * plato/graph/structure/dcsc.hpp:48-49 "vertexId must be compacted" and
+ * plato/graph/partition/sequence.hpp:67).  Internally the engine may renumber
+ * vertices (PLATO_GRAPH_RELABEL); every result crosses the ABI in caller ids.
+ *
+ * Numeric conventions (parity with the reference):
+ *  - PageRank ranks are returned normalised: initial rank 1/V, teleport
+ *    (1-d)/V.  The reference (plato/algo/pagerank/pagerank.hpp:90-146) starts
+ *    at 1.0 with teleport (1-d); every iterate of the reference equals ours
+ *    times V.  opts->eps keeps the reference's units (the sum of rank changes
+ *    over the un-normalised ranks), so early exit triggers on the same
+ *    iteration in exact arithmetic.
+ *  - Personalized PageRank is already normalised in the reference
+ *    (plato/algo/ppr/personalized_pagerank.hpp:71-81): values are returned as is.
+ *  - BFS levels are exact; unreached vertices get PLATO_LEVEL_UNREACHED;
+ *    parents use the reference's invalid marker max_v_i + 1
+ *    (plato/algo/bfs/bfs.hpp:79).
+ */
+#ifndef PLATO_B200_H
+#define PLATO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PLATO_OK          0
+#define PLATO_EINVAL      1  /* bad argument (null pointer, id out of range, ...) */
+#define PLATO_ENOMEM      2  /* device or host allocation failed / over budget     */
+#define PLATO_ECUDA       3  /* a CUDA runtime call failed                          */
+#define PLATO_ETIMEDOUT   4  /* a bounded device wait ran out                       */
+#define PLATO_EBUSY       5  /* server full: no slot or HBM budget for the request  */
+#define PLATO_ENOTFOUND   6  /* nothing ready / unknown request id                  */
+
+#define PLATO_LEVEL_UNREACHED 0xFFFFFFFFu
+
+/* graph creation flags */
+#define PLATO_GRAPH_RELABEL 0x1u /* renumber vertices by descending out-degree inside the engine */
+
+/* personalized pagerank modes */
+#define PLATO_PPR_PULL      0 /* pull-only engine: personalized_pagerank.hpp:40-134     */
+#define PLATO_PPR_PUSHPULL  1 /* push until active edges > E/20, then pull: :137-275   */
+
+typedef uint32_t plato_vid_t; /* plato/graph/base.hpp vid_t */
+typedef uint64_t plato_eid_t; /* plato/graph/base.hpp eid_t */
+
+typedef struct plato_graph plato_graph;
+typedef struct plato_server plato_server;
+
+/* Mirrors graph_info_t (plato/graph/base.hpp:241-257). */
+typedef struct {
+  int32_t     is_directed;
+  plato_vid_t vertices;  /* number of vertices (ids are [0, vertices)) */
+  plato_eid_t edges;     /* input edges; undirected edges count once   */
+  plato_vid_t max_v_i;   /* largest vertex id == vertices - 1          */
+} plato_graph_info;
+
+/* Mirrors pagerank_opts_t (plato/algo/pagerank/pagerank.hpp:39-46). */
+typedef struct {
+  uint32_t iteration;
+  double   damping;
+  double   eps;        /* 0 forces `iteration` epochs */
+} plato_pagerank_opts;
+
+/* Mirrors personalized_pagerank_opts_t (plato/algo/ppr/personalized_pagerank.hpp:18-26). */
+typedef struct {
+  uint32_t    iteration;
+  double      damping;
+  plato_vid_t src;
+  double      eps;
+} plato_ppr_opts;
+
+/* Mirrors bfs_opts_t (plato/algo/bfs/bfs.hpp:37-39). */
+typedef struct {
+  plato_vid_t root;
+} plato_bfs_opts;
+
+/* Mirrors dualmode_engine_opts_t (plato/engine/dualmode.hpp:41-43). */
+typedef struct {
+  double push_threshold; /* push iff active_edges / edges < push_threshold (default 0.05) */
+} plato_dualmode_opts;
+
+/* Per-run statistics (the reference logs the same per epoch, e.g. pagerank.hpp:141-144). */
+typedef struct {
+  uint32_t iterations;      /* epochs executed (including the final non-dividing one) */
+  uint32_t push_iterations; /* epochs run in push mode                                */
+  uint32_t pull_iterations; /* epochs run in pull mode                                */
+  uint32_t reserved;
+  double   delta;           /* last delta (reference units)                           */
+  uint64_t visited;         /* BFS: visited vertex count (bfs.hpp:153-154)            */
+  uint64_t mode_trace;      /* bit i set = epoch i ran in push mode (first 64 epochs) */
+} plato_run_stats;
+
+/* Raw device view of a resident graph in the engine's internal vertex order,
+ * for header-only device code (include/plato_b200/dualmode.cuh). */
+typedef struct {
+  plato_vid_t        vertices;
+  int32_t            is_directed;
+  plato_eid_t        edges;        /* graph_info.edges (input edges)              */
+  plato_eid_t        stored_edges; /* directed edges stored (2*edges undirected)  */
+  const uint64_t*    in_offsets;   /* [V+1] CSC (DCSC without the empty-column compression) */
+  const plato_vid_t* in_adj;       /* [stored_edges] sources, ascending per column */
+  const uint64_t*    out_offsets;  /* [V+1] CSR */
+  const plato_vid_t* out_adj;      /* [stored_edges] destinations, ascending per row */
+  const uint32_t*    out_degree;   /* [V] */
+  const uint32_t*    in_degree;    /* [V] */
+  const plato_vid_t* to_internal;  /* [V] caller id -> internal id (NULL if identity) */
+  const plato_vid_t* to_external;  /* [V] internal id -> caller id (NULL if identity) */
+} plato_graph_device_view;
+
+/* ---- errors / diagnostics ---------------------------------------------- */
+const char* plato_last_error(void);
+/* Number of kernels this library has launched in this process. */
+uint64_t    plato_kernel_launches(void);
+/* Library version string. */
+const char* plato_version(void);
+
+/* ---- kernel timing ---------------------------------------------------------
+ * When enabled, the hot kernels are bracketed by CUDA events on their launch
+ * stream (the device analogue of the reference's per-epoch stop_watch_t,
+ * plato/util/perf.hpp:71-103).  plato_profile_read synchronises those events
+ * and returns the summed device time and launch count of one kernel name
+ * since the last reset. */
+int plato_profile_enable(int on);
+int plato_profile_reset(void);
+int plato_profile_read(const char* kernel, double* total_ms, uint64_t* launches);
+
+/* ---- graph ---------------------------------------------------------------
+ * Replaces create_dualmode_seq_from_path (plato/graph/structure.hpp:983-1086)
+ * for an edge list already in memory: builds CSC (in-edges, the DCSC of
+ * dcsc.hpp:148-152) and CSR (out-edges, the BCSR of bcsr.hpp:167-174) in HBM.
+ * Undirected input is stored in both directions (dcsc.hpp:365-385).  Host
+ * arrays src/dst hold info->edges entries.  Ids >= info->vertices -> EINVAL. */
+int plato_graph_create(const plato_graph_info* info, const plato_vid_t* src,
+                       const plato_vid_t* dst, uint32_t flags, plato_graph** out);
+int plato_graph_destroy(plato_graph* g);
+int plato_graph_get_info(const plato_graph* g, plato_graph_info* info);
+int plato_graph_get_device_view(const plato_graph* g, plato_graph_device_view* view);
+/* Out-degrees computed from the in-edge structure, in caller ids
+ * (generate_dense_out_degrees_fg, plato/graph/structure.hpp:291-346). */
+int plato_graph_out_degrees(plato_graph* g, uint32_t* degrees_out /* host [V] */);
+/* Bytes of HBM held by the graph. */
+int plato_graph_device_bytes(const plato_graph* g, uint64_t* bytes);
+
+/* ---- algorithms (host output buffers) ------------------------------------ */
+/* algo::pagerank (plato/algo/pagerank/pagerank.hpp:60-149).  ranks: host [V]. */
+int plato_pagerank(plato_graph* g, const plato_pagerank_opts* opts, float* ranks,
+                   plato_run_stats* stats);
+/* algo::personalized_pagerank, pull-only (personalized_pagerank.hpp:40-134) or
+ * dual-mode (:137-275) by `mode`.  ranks: host [V]. */
+int plato_personalized_pagerank(plato_graph* g, const plato_ppr_opts* opts, int mode,
+                                float* ranks, plato_run_stats* stats);
+/* algo::breadth_first_search (plato/algo/bfs/bfs.hpp:55-155) with the engine's
+ * push/pull switch (dualmode.hpp:245-297).  levels/parents: host [V] or NULL. */
+int plato_bfs(plato_graph* g, const plato_bfs_opts* opts, const plato_dualmode_opts* engine_opts,
+              uint32_t* levels, plato_vid_t* parents, plato_run_stats* stats);
+
+/* ---- algorithms (device output buffers, caller's CUDA stream) ------------- */
+/* Same as plato_pagerank but writes the ranks to device memory d_ranks [V]
+ * (caller ids) on `stream` (a cudaStream_t; NULL = legacy default stream).
+ * With opts->eps == 0 nothing is read back and the call does not synchronise. */
+int plato_pagerank_device(plato_graph* g, const plato_pagerank_opts* opts, float* d_ranks,
+                          void* stream, plato_run_stats* stats);
+
+/* ---- batched multi-source personalized pagerank --------------------------
+ * K queries, query q's seed set is seeds[seed_offsets[q] .. seed_offsets[q+1]).
+ * Each query follows the seed-set semantics of algo::trustrank
+ * (plato/algo/trustrank/trustrank.hpp:197-245: init 1/|S| on seeds, teleport
+ * (1-d)/|S| on seeds); a query stops once its own L1 delta < eps (plus the
+ * reference's one final non-dividing epoch, pagerank.hpp:137-139). */
+typedef struct {
+  uint32_t max_iterations;
+  double   damping;
+  double   eps;
+  uint32_t topk;       /* 0 = no top-k */
+  uint32_t k_tile;     /* 0 = autotune */
+} plato_ppr_batch_opts;
+
+int plato_ppr_batch(plato_graph* g, uint32_t K, const uint64_t* seed_offsets /* host [K+1] */,
+                    const plato_vid_t* seeds /* host */, const plato_ppr_batch_opts* opts,
+                    float* ranks /* host [K*V] query-major, or NULL */,
+                    plato_vid_t* topk_ids /* host [K*topk] or NULL */,
+                    float* topk_vals /* host [K*topk] or NULL */,
+                    uint32_t* iterations /* host [K] or NULL */);
+
+/* ---- continuous-batching PPR server -------------------------------------- */
+typedef struct {
+  uint32_t max_slots;        /* upper bound of live queries (columns)            */
+  uint64_t hbm_budget_bytes; /* admission budget for per-query state             */
+  uint32_t max_iterations;
+  double   damping;
+  double   eps;
+  uint32_t topk;
+} plato_server_opts;
+
+int plato_server_create(plato_graph* g, const plato_server_opts* opts, plato_server** out);
+/* Queue a request (seed set of n caller ids). Returns its id. */
+int plato_server_submit(plato_server* s, const plato_vid_t* seeds, uint32_t n,
+                        uint64_t* request_id);
+/* Run one engine step: admit queued requests into free slots, run one
+ * iteration over all live slots, retire converged ones. */
+int plato_server_step(plato_server* s);
+/* Fetch one finished result (any request). PLATO_ENOTFOUND if none is ready. */
+int plato_server_poll(plato_server* s, uint64_t* request_id, plato_vid_t* topk_ids,
+                      float* topk_vals, uint32_t* iterations);
+/* live = queries on the device, queued = waiting for admission. */
+int plato_server_stats(const plato_server* s, uint32_t* live, uint32_t* queued,
+                       uint64_t* completed);
+int plato_server_destroy(plato_server* s);
+
+/* ---- synthetic input ------------------------------------------------------
+ * Seeded RMAT edge list (Chakrabarti et al. 2004), self-loops and duplicates
+ * removed, ids compacted to [0, V) (required by the reference, see above),
+ * optionally symmetrised (one entry per unordered pair, is_directed = 0) and
+ * optionally relabelled by a seeded permutation.  Host-side, multithreaded. */
+typedef struct {
+  uint32_t scale;
+  uint32_t edgefactor;
+  uint64_t seed;
+  double   a, b, c;   /* d = 1 - a - b - c */
+  int32_t  symmetrize;
+  int32_t  permute;
+} plato_rmat_params;
+
+typedef struct plato_edge_list plato_edge_list;
+int plato_rmat_generate(const plato_rmat_params* p, plato_edge_list** out);
+int plato_edge_list_info(const plato_edge_list* el, plato_vid_t* vertices, uint64_t* edges);
+/* Pointers stay valid until plato_edge_list_free. Edges are sorted by (src, dst). */
+int plato_edge_list_data(const plato_edge_list* el, const plato_vid_t** src,
+                         const plato_vid_t** dst);
+int plato_edge_list_free(plato_edge_list* el);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* PLATO_B200_H */

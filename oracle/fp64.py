@@ -1,0 +1,101 @@
+"""Independent FP64 oracle — TEST INFRASTRUCTURE ONLY.
+
+Plain scipy.sparse power iteration and a serial level-synchronous BFS, written
+from the mathematical definitions (no engine, no push/pull), used to
+cross-check both ref_cpu.c and the CUDA path:
+
+  PageRank (plato/algo/pagerank/pagerank.hpp:81-146, un-normalised):
+      r_0 = 1;  r_{t+1}(v) = (1-d) + d * sum_{u in in(v)} r_t(u) / deg(u)
+      (deg(u) = out-degree; u with deg 0 has no out-edges, so it never
+      contributes), and the last epoch returns r, earlier epochs feed r/deg.
+  Seed-set PPR (trustrank.hpp:197-245): teleport (1-d)/|S| on seeds, r_0 = 1/|S| on seeds.
+  BFS levels: distance in hops from the root over out-edges.
+"""
+from __future__ import annotations
+
+from collections import deque
+
+import numpy as np
+import scipy.sparse as sp
+
+
+def adjacency(vertices: int, src, dst, is_directed: bool = True) -> sp.csr_matrix:
+    """A[v, u] = number of edges u -> v (in-edge matrix, CSR by destination)."""
+    src = np.asarray(src, dtype=np.int64)
+    dst = np.asarray(dst, dtype=np.int64)
+    if not is_directed:
+        src, dst = np.concatenate([src, dst]), np.concatenate([dst, src])
+    data = np.ones(src.size, dtype=np.float64)
+    return sp.csr_matrix((data, (dst, src)), shape=(vertices, vertices))
+
+
+def _power(A: sp.csr_matrix, x0: np.ndarray, tele: np.ndarray, d: float, iterations: int,
+           eps: float) -> tuple[np.ndarray, int]:
+    deg = np.asarray(A.sum(axis=0)).ravel()  # out-degree (column sums)
+    safe = np.where(deg > 0, deg, 1.0)
+    x = np.where(deg > 0, x0 / safe, x0)
+    epochs = 0
+    it = 0
+    while it < iterations:
+        y = A @ x
+        r = tele + d * y
+        epochs += 1
+        if it == iterations - 1:
+            return r, epochs
+        xn = np.where(deg > 0, r / safe, r)
+        delta = float(np.sum(np.where(deg > 0, np.abs(xn - x) * deg, np.abs(xn - x))))
+        x = xn
+        if eps > 0.0 and delta < eps:
+            it = iterations - 1
+            continue
+        it += 1
+    return x, epochs
+
+
+def pagerank(vertices: int, src, dst, is_directed=True, iterations=100, damping=0.85, eps=0.0):
+    """Reference units (initial rank 1, teleport 1-d) -> (ranks, epochs)."""
+    A = adjacency(vertices, src, dst, is_directed)
+    return _power(A, np.ones(vertices), np.full(vertices, 1.0 - damping), damping, iterations, eps)
+
+
+def ppr(vertices: int, src, dst, source: int, is_directed=True, iterations=100, damping=0.85,
+        eps=0.0):
+    A = adjacency(vertices, src, dst, is_directed)
+    x0 = np.zeros(vertices)
+    x0[source] = 1.0
+    tele = np.zeros(vertices)
+    tele[source] = 1.0 - damping
+    return _power(A, x0, tele, damping, iterations, eps)
+
+
+def seedset_ppr(vertices: int, src, dst, seeds, is_directed=True, iterations=100, damping=0.85,
+                eps=0.0):
+    A = adjacency(vertices, src, dst, is_directed)
+    s = np.unique(np.asarray(seeds, dtype=np.int64))
+    x0 = np.zeros(vertices)
+    x0[s] = 1.0 / s.size
+    tele = np.zeros(vertices)
+    tele[s] = (1.0 - damping) / s.size
+    return _power(A, x0, tele, damping, iterations, eps)
+
+
+def bfs_levels(vertices: int, src, dst, root: int, is_directed=True) -> np.ndarray:
+    src = np.asarray(src, dtype=np.int64)
+    dst = np.asarray(dst, dtype=np.int64)
+    if not is_directed:
+        src, dst = np.concatenate([src, dst]), np.concatenate([dst, src])
+    order = np.argsort(src, kind="stable")
+    s, d = src[order], dst[order]
+    off = np.zeros(vertices + 1, dtype=np.int64)
+    np.add.at(off, s + 1, 1)
+    off = np.cumsum(off)
+    lev = np.full(vertices, 0xFFFFFFFF, dtype=np.uint32)
+    lev[root] = 0
+    q = deque([root])
+    while q:
+        u = q.popleft()
+        for v in d[off[u]:off[u + 1]]:
+            if lev[v] == 0xFFFFFFFF:
+                lev[v] = lev[u] + 1
+                q.append(v)
+    return lev

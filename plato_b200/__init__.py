@@ -1,0 +1,270 @@
+"""plato_b200 — B200-native dual-mode push/pull graph engine (host-side mirror).
+
+Python mirror of the reference's operator surface for the hot path, over the C
+ABI of ``include/plato_b200.h``:
+
+* option structs ``pagerank_opts_t``, ``personalized_pagerank_opts_t``,
+  ``bfs_opts_t``, ``dualmode_engine_opts_t`` with the reference's field names
+  and defaults (plato/algo/pagerank/pagerank.hpp:39-46,
+  plato/algo/ppr/personalized_pagerank.hpp:18-26, plato/algo/bfs/bfs.hpp:37-39,
+  plato/engine/dualmode.hpp:41-43);
+* ``pagerank``, ``personalized_pagerank``, ``breadth_first_search`` with the
+  reference's argument meaning and return values (ranks in reference units,
+  visited count for BFS);
+* ``Graph`` — a resident single-partition graph in HBM (``graph_info_t`` via
+  ``Graph.info``).
+
+Every call runs the CUDA kernels of libplato_b200.so; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import (PLATO_GRAPH_RELABEL, PLATO_LEVEL_UNREACHED, PLATO_PPR_PULL, PLATO_PPR_PUSHPULL,
+                   PlatoError, check, load)
+
+__all__ = [
+    "Graph", "GraphInfo", "PlatoError", "rmat", "pagerank", "personalized_pagerank",
+    "breadth_first_search", "pagerank_opts_t", "personalized_pagerank_opts_t", "bfs_opts_t",
+    "dualmode_engine_opts_t", "PLATO_LEVEL_UNREACHED", "PLATO_PPR_PULL", "PLATO_PPR_PUSHPULL",
+    "kernel_launches",
+]
+
+
+@dataclass
+class pagerank_opts_t:  # noqa: N801 — reference name
+    iteration_: int = 100
+    damping_: float = 0.85
+    eps_: float = 0.001
+
+
+@dataclass
+class personalized_pagerank_opts_t:  # noqa: N801
+    iteration_: int = 100
+    damping_: float = 0.85
+    src_: int = 0
+    eps_: float = 0.001
+
+
+@dataclass
+class bfs_opts_t:  # noqa: N801
+    root_: int = 0
+
+
+@dataclass
+class dualmode_engine_opts_t:  # noqa: N801
+    push_threshold_: float = 0.05
+
+
+@dataclass
+class GraphInfo:
+    """graph_info_t (plato/graph/base.hpp:241-257)."""
+    is_directed_: bool
+    vertices_: int
+    edges_: int
+    max_v_i_: int
+
+
+@dataclass
+class RunStats:
+    iterations: int = 0
+    push_iterations: int = 0
+    pull_iterations: int = 0
+    delta: float = 0.0
+    visited: int = 0
+    mode_trace: list = field(default_factory=list)  # "push"/"pull" per epoch (first 64)
+
+    @classmethod
+    def from_c(cls, s: _lib.RunStats) -> "RunStats":
+        n = min(int(s.iterations), 64)
+        trace = ["push" if (int(s.mode_trace) >> i) & 1 else "pull" for i in range(n)]
+        return cls(int(s.iterations), int(s.push_iterations), int(s.pull_iterations),
+                   float(s.delta), int(s.visited), trace)
+
+
+def kernel_launches() -> int:
+    return int(load().plato_kernel_launches())
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+def rmat(scale: int, edgefactor: int = 16, seed: int = 1, a: float = 0.57, b: float = 0.19,
+         c: float = 0.19, symmetrize: bool = False, permute: bool = False):
+    """Seeded RMAT edge list -> (V, src, dst) numpy uint32 arrays sorted by (src, dst).
+
+    Self-loops and duplicates removed, ids compacted to [0, V); symmetrised
+    graphs keep one (min, max) entry per unordered pair."""
+    lib = load()
+    p = _lib.RmatParams(scale, edgefactor, seed, a, b, c, int(symmetrize), int(permute))
+    h = C.c_void_p()
+    check(lib.plato_rmat_generate(C.byref(p), C.byref(h)), "plato_rmat_generate")
+    try:
+        V = C.c_uint32()
+        E = C.c_uint64()
+        check(lib.plato_edge_list_info(h, C.byref(V), C.byref(E)), "plato_edge_list_info")
+        ps, pd = C.c_void_p(), C.c_void_p()
+        check(lib.plato_edge_list_data(h, C.byref(ps), C.byref(pd)), "plato_edge_list_data")
+        n = int(E.value)
+        src = np.empty(n, dtype=np.uint32)
+        dst = np.empty(n, dtype=np.uint32)
+        if n:
+            C.memmove(src.ctypes.data, ps.value, 4 * n)
+            C.memmove(dst.ctypes.data, pd.value, 4 * n)
+        return int(V.value), src, dst
+    finally:
+        lib.plato_edge_list_free(h)
+
+
+class Graph:
+    """A graph resident in HBM: CSC (in-edges) + CSR (out-edges), single partition.
+
+    Replaces create_dualmode_seq_from_path (plato/graph/structure.hpp:983-1086)
+    for an in-memory edge list.  ``relabel`` lets the engine renumber vertices
+    internally by out-degree; results always come back in caller ids."""
+
+    def __init__(self, vertices: int, src, dst, is_directed: bool = True, relabel: bool = True):
+        self._lib = load()
+        src = _u32(src)
+        dst = _u32(dst)
+        if src.shape != dst.shape:
+            raise ValueError("src and dst must have the same length")
+        info = _lib.GraphInfo(1 if is_directed else 0, int(vertices), int(src.size),
+                              max(int(vertices) - 1, 0))
+        h = C.c_void_p()
+        check(self._lib.plato_graph_create(C.byref(info), _ptr(src), _ptr(dst),
+                                           PLATO_GRAPH_RELABEL if relabel else 0, C.byref(h)),
+              "plato_graph_create")
+        self._h = h
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.plato_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if not self._h:
+            raise ValueError("graph is closed")
+        return self._h
+
+    # -- info ---------------------------------------------------------------
+    @property
+    def info(self) -> GraphInfo:
+        i = _lib.GraphInfo()
+        check(self._lib.plato_graph_get_info(self.handle, C.byref(i)), "plato_graph_get_info")
+        return GraphInfo(bool(i.is_directed), int(i.vertices), int(i.edges), int(i.max_v_i))
+
+    @property
+    def vertices(self) -> int:
+        return self.info.vertices_
+
+    def device_view(self) -> _lib.GraphDeviceView:
+        v = _lib.GraphDeviceView()
+        check(self._lib.plato_graph_get_device_view(self.handle, C.byref(v)),
+              "plato_graph_get_device_view")
+        return v
+
+    def device_bytes(self) -> int:
+        b = C.c_uint64()
+        check(self._lib.plato_graph_device_bytes(self.handle, C.byref(b)), "plato_graph_device_bytes")
+        return int(b.value)
+
+    def out_degrees(self) -> np.ndarray:
+        out = np.empty(self.vertices, dtype=np.uint32)
+        check(self._lib.plato_graph_out_degrees(self.handle, _ptr(out)), "plato_graph_out_degrees")
+        return out
+
+    # -- algorithms (normalised FP32 outputs) -------------------------------
+    def pagerank(self, iteration: int = 100, damping: float = 0.85, eps: float = 0.0):
+        """Normalised ranks (sum ~ 1; the reference's values are these times V)."""
+        out = np.empty(self.vertices, dtype=np.float32)
+        o = _lib.PagerankOpts(iteration, damping, eps)
+        s = _lib.RunStats()
+        check(self._lib.plato_pagerank(self.handle, C.byref(o), _ptr(out), C.byref(s)),
+              "plato_pagerank")
+        return out, RunStats.from_c(s)
+
+    def pagerank_device(self, d_out: int, iteration: int, damping: float = 0.85,
+                        eps: float = 0.0, stream: int = 0):
+        """PageRank into device memory `d_out` (a CUDA pointer) on `stream`."""
+        o = _lib.PagerankOpts(iteration, damping, eps)
+        s = _lib.RunStats()
+        check(self._lib.plato_pagerank_device(self.handle, C.byref(o), C.c_void_p(d_out),
+                                              C.c_void_p(stream), C.byref(s)),
+              "plato_pagerank_device")
+        return RunStats.from_c(s)
+
+    def personalized_pagerank(self, src: int, iteration: int = 100, damping: float = 0.85,
+                              eps: float = 0.0, mode: int = PLATO_PPR_PULL):
+        out = np.empty(self.vertices, dtype=np.float32)
+        o = _lib.PprOpts(iteration, damping, src, eps)
+        s = _lib.RunStats()
+        check(self._lib.plato_personalized_pagerank(self.handle, C.byref(o), mode, _ptr(out),
+                                                    C.byref(s)),
+              "plato_personalized_pagerank")
+        return out, RunStats.from_c(s)
+
+    def bfs(self, root: int, push_threshold: float = 0.05, parents: bool = True):
+        """-> (levels uint32 [V] with PLATO_LEVEL_UNREACHED, parents or None, stats)."""
+        V = self.vertices
+        lev = np.empty(V, dtype=np.uint32)
+        par = np.empty(V, dtype=np.uint32) if parents else None
+        o = _lib.BfsOpts(root)
+        eo = _lib.DualmodeOpts(push_threshold)
+        s = _lib.RunStats()
+        check(self._lib.plato_bfs(self.handle, C.byref(o), C.byref(eo), _ptr(lev),
+                                  _ptr(par) if parents else None, C.byref(s)), "plato_bfs")
+        return lev, par, RunStats.from_c(s)
+
+
+# ---- reference-shaped entry points -------------------------------------------
+
+def pagerank(graph: Graph, opts: pagerank_opts_t | None = None) -> np.ndarray:
+    """algo::pagerank (plato/algo/pagerank/pagerank.hpp:60-149): ranks in the
+    reference's units (initial rank 1.0, teleport 1-d), float64 array [V]."""
+    opts = opts or pagerank_opts_t()
+    r, _ = graph.pagerank(opts.iteration_, opts.damping_, opts.eps_)
+    return r.astype(np.float64) * graph.vertices
+
+
+def personalized_pagerank(graph: Graph, opts: personalized_pagerank_opts_t | None = None,
+                          pushpull: bool = False) -> np.ndarray:
+    """algo::personalized_pagerank: the pull-only overload
+    (personalized_pagerank.hpp:40-134) or, with pushpull=True, the dual-mode
+    overload taking in- and out-edges (:137-275)."""
+    opts = opts or personalized_pagerank_opts_t()
+    r, _ = graph.personalized_pagerank(opts.src_, opts.iteration_, opts.damping_, opts.eps_,
+                                       PLATO_PPR_PUSHPULL if pushpull else PLATO_PPR_PULL)
+    return r.astype(np.float64)
+
+
+def breadth_first_search(graph: Graph, opts: bfs_opts_t | None = None,
+                         engine_opts: dualmode_engine_opts_t | None = None) -> int:
+    """algo::breadth_first_search (plato/algo/bfs/bfs.hpp:55-155): visited count."""
+    opts = opts or bfs_opts_t()
+    eo = engine_opts or dualmode_engine_opts_t()
+    _, _, st = graph.bfs(opts.root_, eo.push_threshold_, parents=False)
+    return st.visited

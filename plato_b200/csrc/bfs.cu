@@ -1,0 +1,234 @@
+// Breadth-first search with the dual-mode engine's push/pull switch.
+//
+// Mirrors algo::breadth_first_search (plato/algo/bfs/bfs.hpp:55-155) driven by
+// dualmode_engine_t::foreach_edges (plato/engine/dualmode.hpp:245-297):
+//   each epoch: active_edges = sum of out-degrees of the current frontier;
+//   push iff active_edges / edges < push_threshold (edges doubled for
+//   undirected graphs, dualmode.hpp:261-262), else pull.
+//   push (bfs.hpp:97-118): each frontier vertex claims unvisited out-neighbours.
+//   pull (bfs.hpp:119-136): each unvisited vertex takes the first in-neighbour
+//   that is in the current frontier.
+// A vertex first reached in epoch e has level e + 1 (root: 0).  Levels are
+// unique; parents depend on claim order in push mode, as in the reference.
+#include <new>
+
+#include "graph.cuh"
+#include "push.cuh"
+
+namespace plato_b200 {
+
+struct bfs_workspace {
+  push_frontier fr[2];
+  dbuf<uint32_t> visited;
+  dbuf<uint32_t> level, parent;
+};
+
+void destroy_bfs_workspace(bfs_workspace* ws) { delete ws; }
+
+namespace {
+
+__global__ void k_bfs_init(uint32_t V, uint32_t root, uint32_t invalid_parent, uint32_t* level,
+                           uint32_t* parent, uint32_t* visited) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    level[v] = v == root ? 0u : PLATO_LEVEL_UNREACHED;
+    parent[v] = v == root ? root : invalid_parent;
+    if ((v & 31) == 0) {
+      uint32_t w = 0;
+      if ((root >> 5) == (v >> 5)) w = 1u << (root & 31);
+      visited[v >> 5] = w;
+    }
+  }
+}
+
+// Push level: frontier chunks -> claim unvisited out-neighbours.
+__global__ void __launch_bounds__(256) k_bfs_push(frontier_view cur, unsigned long long nchunks,
+                                                  frontier_view next,
+                                                  const uint64_t* __restrict__ out_off,
+                                                  const uint32_t* __restrict__ out_adj,
+                                                  const uint32_t* __restrict__ deg,
+                                                  uint32_t* visited, uint32_t* level,
+                                                  uint32_t* parent, uint32_t new_level) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t c = warp; c < nchunks; c += nwarps) {
+    const uint2 ch = cur.chunks[c];
+    const uint32_t u = ch.x;
+    const uint64_t b = out_off[u] + static_cast<uint64_t>(ch.y) * kPushChunk;
+    const uint64_t e_end = min(b + kPushChunk, out_off[u + 1]);
+    for (uint64_t base = b; base < e_end; base += 32) {
+      const uint64_t e = base + lane;
+      uint32_t dst = 0;
+      bool fresh = false;
+      if (e < e_end) {
+        dst = out_adj[e];
+        const uint32_t bit = 1u << (dst & 31);
+        if (!(visited[dst >> 5] & bit)) fresh = !(atomicOr(&visited[dst >> 5], bit) & bit);
+        if (fresh) {
+          level[dst] = new_level;
+          parent[dst] = u;
+          atomicOr(&next.bits[dst >> 5], bit);
+        }
+      }
+      frontier_append_warp(next, fresh, dst, deg);
+    }
+  }
+}
+
+// Pull level: every unvisited vertex scans its in-edges for a frontier member.
+__global__ void __launch_bounds__(256) k_bfs_pull(uint32_t V, frontier_view cur, frontier_view next,
+                                                  const uint64_t* __restrict__ in_off,
+                                                  const uint32_t* __restrict__ in_adj,
+                                                  const uint32_t* __restrict__ deg,
+                                                  uint32_t* visited, uint32_t* level,
+                                                  uint32_t* parent, uint32_t new_level) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t nrounds = (V + stride - 1) / stride;
+  for (uint64_t r = 0; r < nrounds; ++r) {  // warp-uniform trip count for the appends
+    const uint64_t v = r * stride + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    bool fresh = false;
+    if (v < V && !test_bit(visited, static_cast<uint32_t>(v))) {
+      const uint64_t b = in_off[v], e = in_off[v + 1];
+      for (uint64_t i = b; i < e; ++i) {
+        const uint32_t s = in_adj[i];
+        if (test_bit(cur.bits, s)) {
+          fresh = true;
+          level[v] = new_level;
+          parent[v] = s;
+          const uint32_t bit = 1u << (v & 31);
+          atomicOr(&visited[v >> 5], bit);
+          atomicOr(&next.bits[v >> 5], bit);
+          break;
+        }
+      }
+    }
+    frontier_append_warp(next, fresh, static_cast<uint32_t>(v), deg);
+  }
+}
+
+int ensure_bfs_ws(plato_graph* g) {
+  if (!g->bfs_ws) {
+    g->bfs_ws = new (std::nothrow) bfs_workspace();
+    if (!g->bfs_ws) return set_error(PLATO_ENOMEM, "bfs workspace: host allocation failed");
+  }
+  bfs_workspace* ws = g->bfs_ws;
+  const uint32_t V = g->info.vertices;
+  PLATO_TRY(frontier_alloc(ws->fr[0], g));
+  PLATO_TRY(frontier_alloc(ws->fr[1], g));
+  PLATO_TRY(ws->visited.alloc((V + 31) / 32));
+  PLATO_TRY(ws->level.alloc(V));
+  PLATO_TRY(ws->parent.alloc(V));
+  return PLATO_OK;
+}
+
+// parent ids are internal; map to caller ids (the invalid marker stays).
+__global__ void k_parents_to_external(const uint32_t* __restrict__ parent_int,
+                                      const uint32_t* __restrict__ to_ext, uint32_t V,
+                                      uint32_t invalid, uint32_t* parent_ext) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < V;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t p = parent_int[i];
+    parent_ext[to_ext[i]] = (p == invalid) ? invalid : to_ext[p];
+  }
+}
+
+int bfs_impl(plato_graph* g, const plato_bfs_opts* o, const plato_dualmode_opts* eo,
+             cudaStream_t st, plato_run_stats* stats) {
+  const uint32_t V = g->info.vertices;
+  if (o->root >= V) return set_error(PLATO_EINVAL, "bfs: root out of range");
+  const double threshold = eo ? eo->push_threshold : 0.05;
+  PLATO_TRY(ensure_bfs_ws(g));
+  bfs_workspace* ws = g->bfs_ws;
+  uint32_t root = 0;
+  PLATO_TRY(lookup_internal(g, o->root, &root, st));
+  const uint32_t invalid_parent = g->info.max_v_i + 1;  // bfs.hpp:79
+  k_bfs_init<<<grid_for(V, 256), 256, 0, st>>>(V, root, invalid_parent, ws->level.p, ws->parent.p,
+                                                ws->visited.p);
+  PLATO_LAUNCHED("k_bfs_init");
+  PLATO_TRY(frontier_reset(ws->fr[0], V, st));
+  PLATO_TRY(frontier_seed(ws->fr[0], g, root, st));
+  PLATO_TRY(frontier_read(ws->fr[0], st));
+
+  const double edges = static_cast<double>(g->stored_edges);
+  int cur = 0;
+  uint64_t actives = 1, visited = 1, trace = 0;
+  uint32_t epoch = 0, push_epochs = 0;
+  const unsigned pull_blocks = grid_for(V, 256, 148 * 8);
+  while (actives != 0) {
+    push_frontier& fc = ws->fr[cur];
+    push_frontier& fn = ws->fr[cur ^ 1];
+    PLATO_TRY(frontier_reset(fn, V, st));
+    const uint64_t active_edges = fc.h_counters[2];
+    const bool is_sparse = (static_cast<double>(active_edges) / edges) < threshold;
+    if (is_sparse) {
+      const unsigned long long nchunks = fc.h_counters[1];
+      if (nchunks) {
+        k_bfs_push<<<grid_for(nchunks * 32, 256, 148 * 16), 256, 0, st>>>(
+            fc.view(), nchunks, fn.view(), g->out_off.p, g->out_adj.p, g->out_deg.p,
+            ws->visited.p, ws->level.p, ws->parent.p, epoch + 1);
+        PLATO_LAUNCHED("k_bfs_push");
+      }
+      if (epoch < 64) trace |= 1ull << epoch;
+      ++push_epochs;
+    } else {
+      k_bfs_pull<<<pull_blocks, 256, 0, st>>>(V, fc.view(), fn.view(), g->in_off.p, g->in_adj.p,
+                                              g->out_deg.p, ws->visited.p, ws->level.p,
+                                              ws->parent.p, epoch + 1);
+      PLATO_LAUNCHED("k_bfs_pull");
+    }
+    PLATO_TRY(frontier_read(fn, st));
+    actives = fn.h_counters[0];
+    visited += actives;
+    ++epoch;
+    cur ^= 1;
+  }
+  if (stats) {
+    *stats = plato_run_stats{};
+    stats->iterations = epoch;
+    stats->push_iterations = push_epochs;
+    stats->pull_iterations = epoch - push_epochs;
+    stats->visited = visited;
+    stats->mode_trace = trace;
+  }
+  return PLATO_OK;
+}
+
+}  // namespace
+}  // namespace plato_b200
+
+using namespace plato_b200;
+
+extern "C" int plato_bfs(plato_graph* g, const plato_bfs_opts* opts,
+                         const plato_dualmode_opts* engine_opts, uint32_t* levels,
+                         plato_vid_t* parents, plato_run_stats* stats) {
+  if (!g || !opts) return set_error(PLATO_EINVAL, "plato_bfs: null argument");
+  std::lock_guard<std::mutex> lock(g->mu);
+  PLATO_CUDA_TRY(cudaSetDevice(g->device));
+  cudaStream_t st = g->stream;
+  PLATO_TRY(bfs_impl(g, opts, engine_opts, st, stats));
+  const uint32_t V = g->info.vertices;
+  bfs_workspace* ws = g->bfs_ws;
+  if (levels || parents) {
+    dbuf<uint32_t> ext;
+    PLATO_TRY(ext.alloc(V));
+    if (levels) {
+      PLATO_TRY(scatter_to_external_u32(g, ws->level.p, ext.p, st));
+      PLATO_CUDA_TRY(cudaMemcpyAsync(levels, ext.p, V * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+      PLATO_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    if (parents) {
+      if (g->relabeled) {
+        k_parents_to_external<<<grid_for(V, 256), 256, 0, st>>>(
+            ws->parent.p, g->to_ext.p, V, g->info.max_v_i + 1, ext.p);
+        PLATO_LAUNCHED("k_parents_to_external");
+      } else {
+        PLATO_CUDA_TRY(cudaMemcpyAsync(ext.p, ws->parent.p, V * sizeof(uint32_t),
+                                       cudaMemcpyDeviceToDevice, st));
+      }
+      PLATO_CUDA_TRY(cudaMemcpyAsync(parents, ext.p, V * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+      PLATO_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+  }
+  return PLATO_OK;
+}
