@@ -38,6 +38,7 @@ sys.path.insert(0, str(ROOT))
 SCALE, EDGEFACTOR, SEED = 24, 16, 3
 ITERATIONS, DAMPING = 20, 0.85
 METRIC = "PageRank GTEPS (RMAT s24 ef16, 20 iterations, pull)"
+PULL_KERNEL = "k_pull_warp"  # dominant kernel of a PageRank step
 
 
 def env_rank():
@@ -216,9 +217,9 @@ def run_plato(args):
     import ctypes as C
     tot = C.c_double()
     cnt = C.c_uint64()
-    lib.plato_profile_read(b"k_pull_merge", C.byref(tot), C.byref(cnt))
+    lib.plato_profile_read(PULL_KERNEL.encode(), C.byref(tot), C.byref(cnt))
     merge_ms, merge_n = tot.value, int(cnt.value)
-    lib.plato_profile_read(b"k_pull_fixup", C.byref(tot), C.byref(cnt))
+    lib.plato_profile_read((PULL_KERNEL + "_fixup").encode(), C.byref(tot), C.byref(cnt))
     fix_ms = tot.value
     ms = ev0.elapsed_time(ev1) / args.steps
     if dist:
@@ -260,11 +261,11 @@ def run_plato(args):
     per_launch_ms = merge_ms / max(merge_n, 1)
     achieved = bytes_per_launch / (per_launch_ms / 1e3) / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None, "kernel": "k_pull_merge",
+            "frac": achieved / peak, "traffic": None, "kernel": PULL_KERNEL,
             "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
             "bytes_per_launch": bytes_per_launch, "launch_ms": per_launch_ms,
             "fixup_ms_per_launch": fix_ms / max(merge_n, 1)}
-    prof = ROOT / "profiles" / "pull_merge_rmat_s24_traffic.json"
+    prof = ROOT / "profiles" / "k_pull_warp_rmat_s24_traffic.json"
     if prof.exists():
         tr = json.loads(prof.read_text())
         roof["traffic"] = tr.get("dram_bytes_per_launch_full")
@@ -305,7 +306,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["plato", "reference"], default="plato")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scale", type=int, default=SCALE,
+                    help="RMAT scale (smaller values are for profiling captures only)")
     args = ap.parse_args()
+    globals()["SCALE"] = args.scale
     if args.impl == "reference":
         return run_reference(args)
     return run_plato(args)

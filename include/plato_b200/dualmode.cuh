@@ -1,0 +1,468 @@
+/*
+ * dualmode.cuh — header-only device form of plato::dualmode_engine_t.
+ *
+ * Mirrors the reference engine (plato/engine/dualmode.hpp:75-166) on a graph
+ * resident in HBM (plato_graph from include/plato_b200.h):
+ *
+ *   plato_b200::dualmode_engine_t engine(graph);            // dualmode.hpp:93-97
+ *   auto rank   = engine.alloc_v_state<double>();           // :232-236
+ *   auto active = engine.alloc_v_subset();                  // :238-242
+ *   R r = engine.foreach_edges<MSG, R>(push_signal, push_slot,
+ *                                      pull_signal, pull_slot, active);  // :245-297
+ *   R r = engine.foreach_edges<MSG, R>(push_signal, push_slot, active);  // push only
+ *   R r = engine.foreach_edges<MSG, R>(pull_signal, pull_slot);          // pull only
+ *
+ * Functors are __device__ (extended) lambdas with the reference's shapes
+ * (dualmode.hpp:119-124):
+ *   push_signal  void(const push_context<MSG>&, vid_t v)        ctx.send(MSG)
+ *   push_slot    R(int p, MSG& msg)
+ *   pull_signal  void(const pull_context<MSG>&, vid_t v, const adj_unit_list_t& adjs)
+ *                                                                ctx.send(mepa_ag_message_t<MSG>)
+ *   pull_slot    R(int p, mepa_ag_message_t<MSG>& msg)
+ * context.send() applies the slot on the device right away (the reference
+ * ships the message through MPI, message_passing.hpp:88-144, :286-335), and
+ * the call returns the sum of the slot returns, like the reference.
+ *
+ * Execution model (what "thread safe" means here, as in the reference where
+ * functors run concurrently on OpenMP threads):
+ *   pull  every vertex with in-edges is visited; its in-adjacency is split into
+ *         chunks of at most kPullChunk edges and each chunk is one signal call,
+ *         exactly like the reference's per-partition pieces of a DCSC column,
+ *         so a vertex may receive several messages and the slot must combine
+ *         them (atomics), as the reference's write_add / CAS slots do.
+ *   push  one signal call per active vertex (thread per vertex, frontier
+ *         compacted with ballot/popc); the slot reaches out-edges through
+ *         engine.out_edges().neighbours(v).
+ *   switch  active_edges = sum of out-degrees over `actives`; push iff
+ *         active_edges / edges < push_threshold, edges doubled for undirected
+ *         graphs (dualmode.hpp:261-279).
+ * Vertex ids seen by functors are the engine's internal ids; states copied to
+ * the host with to_host() are returned in caller ids.
+ */
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "plato_b200.h"
+
+namespace plato_b200 {
+
+using vid_t = uint32_t;
+using eid_t = uint64_t;
+
+constexpr uint32_t kPullChunk = 256;
+
+struct adj_unit_t {  // adj_unit_t<empty_t> (plato/graph/base.hpp)
+  vid_t neighbour_;
+};
+
+struct adj_unit_list_t {  // adj_unit_list_t (plato/graph/base.hpp)
+  const adj_unit_t* begin_;
+  const adj_unit_t* end_;
+};
+
+template <typename MSG>
+struct mepa_ag_message_t {  // plato/graph/message_passing.hpp:47-56
+  vid_t v_i_;
+  MSG message_;
+};
+
+struct dualmode_engine_opts_t {  // plato/engine/dualmode.hpp:41-43
+  double push_threshold_ = 0.05;
+};
+
+inline void check_cuda(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Out-edge view usable inside device functors (bcsr_t::neighbours, bcsr.hpp:225-240).
+struct out_edges_view {
+  const uint64_t* off;
+  const vid_t* adj;
+  __device__ adj_unit_list_t neighbours(vid_t v) const {
+    return adj_unit_list_t{reinterpret_cast<const adj_unit_t*>(adj + off[v]),
+                           reinterpret_cast<const adj_unit_t*>(adj + off[v + 1])};
+  }
+};
+
+// Device bitmap (bitmap_t, plato/util/bitmap.hpp:43-350), 32-bit words.
+class bitmap_t {
+ public:
+  bitmap_t() = default;
+  explicit bitmap_t(uint32_t n) : n_(n) {
+    check_cuda(cudaMalloc(&w_, words() * sizeof(uint32_t)), "bitmap alloc");
+    clear();
+  }
+  bitmap_t(bitmap_t&& o) noexcept : w_(o.w_), n_(o.n_) { o.w_ = nullptr; }
+  bitmap_t& operator=(bitmap_t&& o) noexcept {
+    std::swap(w_, o.w_);
+    std::swap(n_, o.n_);
+    return *this;
+  }
+  bitmap_t(const bitmap_t&) = delete;
+  bitmap_t& operator=(const bitmap_t&) = delete;
+  ~bitmap_t() {
+    if (w_) cudaFree(w_);
+  }
+  size_t words() const { return (static_cast<size_t>(n_) + 31) / 32; }
+  void clear() { check_cuda(cudaMemset(w_, 0, words() * 4), "bitmap clear"); }
+  uint32_t size() const { return n_; }
+  uint32_t* data() const { return w_; }
+  // host-side single bit set (bitmap.hpp:207-222)
+  void set_bit_host(vid_t v) {
+    uint32_t w = 0;
+    check_cuda(cudaMemcpy(&w, w_ + (v >> 5), 4, cudaMemcpyDeviceToHost), "bitmap read");
+    w |= 1u << (v & 31);
+    check_cuda(cudaMemcpy(w_ + (v >> 5), &w, 4, cudaMemcpyHostToDevice), "bitmap write");
+  }
+  // popcount (bitmap.hpp:229-238)
+  uint64_t count() const;
+
+  struct view {
+    uint32_t* w;
+    __device__ void set_bit(vid_t v) const { atomicOr(w + (v >> 5), 1u << (v & 31)); }
+    __device__ bool get_bit(vid_t v) const { return (w[v >> 5] >> (v & 31)) & 1u; }
+  };
+  view dev() const { return view{w_}; }
+
+ private:
+  uint32_t* w_ = nullptr;
+  uint32_t n_ = 0;
+};
+
+// Device vertex state (dense_state_t, plato/graph/state/dense_state.hpp:43-425).
+template <typename T>
+class dense_state_t {
+ public:
+  dense_state_t() = default;
+  explicit dense_state_t(uint32_t n) : n_(n) {
+    check_cuda(cudaMalloc(&p_, sizeof(T) * (n ? n : 1)), "state alloc");
+  }
+  dense_state_t(dense_state_t&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr; }
+  dense_state_t& operator=(dense_state_t&& o) noexcept {
+    std::swap(p_, o.p_);
+    std::swap(n_, o.n_);
+    return *this;
+  }
+  dense_state_t(const dense_state_t&) = delete;
+  dense_state_t& operator=(const dense_state_t&) = delete;
+  ~dense_state_t() {
+    if (p_) cudaFree(p_);
+  }
+  T* data() const { return p_; }
+  uint32_t size() const { return n_; }
+  void fill(const T& v);  // dense_state.hpp:241-254
+  // raw copy in the engine's internal vertex order
+  std::vector<T> to_host_internal() const {
+    std::vector<T> h(n_);
+    check_cuda(cudaMemcpy(h.data(), p_, sizeof(T) * n_, cudaMemcpyDeviceToHost), "state copy");
+    return h;
+  }
+
+ private:
+  T* p_ = nullptr;
+  uint32_t n_ = 0;
+};
+
+namespace detail {
+
+template <typename T>
+__global__ void k_fill(T* p, uint32_t n, T v) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+static __global__ void k_popc(const uint32_t* w, size_t nw, unsigned long long* out) {
+  unsigned long long c = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nw;
+       i += (size_t)gridDim.x * blockDim.x)
+    c += __popc(w[i]);
+  atomicAdd(out, c);
+}
+
+// Frontier compaction + active-edge count (dualmode.hpp:264-277).
+static __global__ void k_compact(const uint32_t* bits, uint32_t n, const uint32_t* deg,
+                                 vid_t* queue, unsigned long long* counters) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t rounds = (n + stride - 1) / stride;
+  for (uint64_t r = 0; r < rounds; ++r) {
+    const uint64_t v = r * stride + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const bool on = v < n && ((bits[v >> 5] >> (v & 31)) & 1u);
+    const unsigned m = __ballot_sync(0xffffffffu, on);
+    unsigned long long base = 0;
+    if (lane == 0 && m) base = atomicAdd(&counters[0], static_cast<unsigned long long>(__popc(m)));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    unsigned long long de = on ? deg[v] : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) de += __shfl_xor_sync(0xffffffffu, de, o);
+    if (lane == 0 && de) atomicAdd(&counters[1], de);
+    if (on) queue[base + __popc(m & ((1u << lane) - 1u))] = static_cast<vid_t>(v);
+  }
+}
+
+// Pull chunk list: (vertex, first edge) for every kPullChunk edges of every column.
+static __global__ void k_count_chunks(const uint64_t* off, uint32_t V, uint32_t* cnt) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+       v += (uint64_t)gridDim.x * blockDim.x)
+    cnt[v] = static_cast<uint32_t>((off[v + 1] - off[v] + kPullChunk - 1) / kPullChunk);
+}
+
+static __global__ void k_fill_chunks(const uint64_t* off, uint32_t V, const uint64_t* cstart,
+                                     uint2* chunks) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t n = (off[v + 1] - off[v] + kPullChunk - 1) / kPullChunk;
+    for (uint64_t k = 0; k < n; ++k) chunks[cstart[v] + k] = make_uint2(static_cast<uint32_t>(v), static_cast<uint32_t>(k));
+  }
+}
+
+template <typename R>
+__device__ inline void reduce_add(R v, R* out) {
+  atomicAdd(out, v);
+}
+
+}  // namespace detail
+
+// Contexts handed to the signal functors.
+template <typename MSG, typename R, typename SLOT>
+struct pull_context {
+  const SLOT* slot;
+  R* acc;
+  __device__ void send(const mepa_ag_message_t<MSG>& m) const {
+    mepa_ag_message_t<MSG> msg = m;
+    *acc += (*slot)(0, msg);
+  }
+};
+
+template <typename MSG, typename R, typename SLOT>
+struct push_context {
+  const SLOT* slot;
+  R* acc;
+  __device__ void send(const MSG& m) const {
+    MSG msg = m;
+    *acc += (*slot)(0, msg);
+  }
+};
+
+namespace detail {
+
+template <typename MSG, typename R, typename SIG, typename SLOT>
+__global__ void k_pull(const uint2* chunks, uint64_t nchunks, const uint64_t* off, const vid_t* adj,
+                       SIG sig, SLOT slot, R* result) {
+  R acc = R();
+  pull_context<MSG, R, SLOT> ctx{&slot, &acc};
+  for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < nchunks;
+       c += (uint64_t)gridDim.x * blockDim.x) {
+    const uint2 ch = chunks[c];
+    const uint64_t b = off[ch.x] + static_cast<uint64_t>(ch.y) * kPullChunk;
+    const uint64_t e = min(b + kPullChunk, off[ch.x + 1]);
+    const adj_unit_list_t adjs{reinterpret_cast<const adj_unit_t*>(adj + b),
+                               reinterpret_cast<const adj_unit_t*>(adj + e)};
+    sig(ctx, static_cast<vid_t>(ch.x), adjs);
+  }
+  if (acc != R()) reduce_add(acc, result);
+}
+
+template <typename MSG, typename R, typename SIG, typename SLOT>
+__global__ void k_push(const vid_t* queue, uint64_t n, SIG sig, SLOT slot, R* result) {
+  R acc = R();
+  push_context<MSG, R, SLOT> ctx{&slot, &acc};
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    sig(ctx, queue[i]);
+  if (acc != R()) reduce_add(acc, result);
+}
+
+}  // namespace detail
+
+template <typename T>
+void dense_state_t<T>::fill(const T& v) {
+  detail::k_fill<T><<<592, 256>>>(p_, n_, v);
+  check_cuda(cudaGetLastError(), "fill");
+}
+
+inline uint64_t bitmap_t::count() const {
+  unsigned long long* d = nullptr;
+  check_cuda(cudaMalloc(&d, sizeof(*d)), "count alloc");
+  cudaMemset(d, 0, sizeof(*d));
+  detail::k_popc<<<296, 256>>>(w_, words(), d);
+  unsigned long long h = 0;
+  check_cuda(cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost), "count read");
+  cudaFree(d);
+  return h;
+}
+
+class dualmode_engine_t {
+ public:
+  explicit dualmode_engine_t(plato_graph* g, dualmode_engine_opts_t opts = dualmode_engine_opts_t())
+      : g_(g), opts_(opts) {
+    if (plato_graph_get_device_view(g, &view_) != PLATO_OK) throw std::runtime_error(plato_last_error());
+    plato_graph_get_info(g, &info_);
+  }
+  dualmode_engine_t(const dualmode_engine_t&) = delete;
+  dualmode_engine_t& operator=(const dualmode_engine_t&) = delete;
+  ~dualmode_engine_t() {
+    if (chunks_) cudaFree(chunks_);
+    if (queue_) cudaFree(queue_);
+    if (counters_) cudaFree(counters_);
+    if (result_) cudaFree(result_);
+  }
+
+  const plato_graph_info& graph_info() const { return info_; }
+  uint32_t vertices() const { return view_.vertices; }
+
+  template <typename T>
+  dense_state_t<T> alloc_v_state() const { return dense_state_t<T>(view_.vertices); }
+  bitmap_t alloc_v_subset() const { return bitmap_t(view_.vertices); }
+
+  out_edges_view out_edges() const {
+    return reversed_ ? out_edges_view{view_.in_offsets, view_.in_adj}
+                     : out_edges_view{view_.out_offsets, view_.out_adj};
+  }
+  const uint32_t* out_degrees() const { return view_.out_degree; }
+  void reverse() { reversed_ = !reversed_; }
+  bool is_reversed() const { return reversed_; }
+
+  // caller id <-> internal id (identity when the graph was not relabelled)
+  vid_t to_internal(vid_t ext) const {
+    if (!view_.to_internal) return ext;
+    vid_t v = 0;
+    check_cuda(cudaMemcpy(&v, view_.to_internal + ext, 4, cudaMemcpyDeviceToHost), "to_internal");
+    return v;
+  }
+  template <typename T>
+  std::vector<T> to_host(const dense_state_t<T>& s) const {
+    std::vector<T> in = s.to_host_internal();
+    if (!view_.to_external) return in;
+    std::vector<vid_t> ext(view_.vertices);
+    check_cuda(cudaMemcpy(ext.data(), view_.to_external, 4ull * view_.vertices, cudaMemcpyDeviceToHost),
+               "to_external");
+    std::vector<T> out(in.size());
+    for (size_t i = 0; i < in.size(); ++i) out[ext[i]] = in[i];
+    return out;
+  }
+
+  // pull only (dualmode.hpp:299-309)
+  template <typename MSG, typename R, typename PULL_SIGNAL, typename PULL_SLOT>
+  R foreach_edges(PULL_SIGNAL signal, PULL_SLOT slot) {
+    ensure_chunks();
+    R* res = result_buf<R>();
+    detail::k_pull<MSG, R><<<grid(nchunks_), 256>>>(chunks_, nchunks_, in_off(), in_adj(), signal,
+                                                     slot, res);
+    check_cuda(cudaGetLastError(), "pull launch");
+    return read_result<R>(res);
+  }
+
+  // push only (dualmode.hpp:311-322)
+  template <typename MSG, typename R, typename PUSH_SIGNAL, typename PUSH_SLOT>
+  R foreach_edges(PUSH_SIGNAL signal, PUSH_SLOT slot, bitmap_t& actives) {
+    uint64_t n = 0, ae = 0;
+    compact(actives, &n, &ae);
+    return push_queue<MSG, R>(signal, slot, n);
+  }
+
+  // push + pull, engine-chosen (dualmode.hpp:245-297)
+  template <typename MSG, typename R, typename PUSH_SIGNAL, typename PUSH_SLOT,
+            typename PULL_SIGNAL, typename PULL_SLOT>
+  R foreach_edges(PUSH_SIGNAL push_signal, PUSH_SLOT push_slot, PULL_SIGNAL pull_signal,
+                  PULL_SLOT pull_slot, bitmap_t& actives) {
+    uint64_t n = 0, active_edges = 0;
+    compact(actives, &n, &active_edges);
+    uint64_t edges = info_.edges;
+    if (!info_.is_directed) edges *= 2;
+    last_push_ = (static_cast<double>(active_edges) / static_cast<double>(edges)) < opts_.push_threshold_;
+    if (last_push_) return push_queue<MSG, R>(push_signal, push_slot, n);
+    return foreach_edges<MSG, R>(pull_signal, pull_slot);
+  }
+
+  bool last_was_push() const { return last_push_; }
+
+ private:
+  const uint64_t* in_off() const { return reversed_ ? view_.out_offsets : view_.in_offsets; }
+  const vid_t* in_adj() const { return reversed_ ? view_.out_adj : view_.in_adj; }
+  static unsigned grid(uint64_t n) {
+    uint64_t b = (n + 255) / 256;
+    if (b < 1) b = 1;
+    if (b > 148 * 16) b = 148 * 16;
+    return static_cast<unsigned>(b);
+  }
+
+  void ensure_chunks() {
+    if (chunks_ && chunks_reversed_ == reversed_) return;
+    if (chunks_) cudaFree(chunks_);
+    const uint32_t V = view_.vertices;
+    uint32_t* cnt = nullptr;
+    uint64_t* start = nullptr;
+    check_cuda(cudaMalloc(&cnt, 4ull * V), "chunks");
+    check_cuda(cudaMalloc(&start, 8ull * (V + 1)), "chunks");
+    detail::k_count_chunks<<<grid(V), 256>>>(in_off(), V, cnt);
+    std::vector<uint32_t> h(V);
+    check_cuda(cudaMemcpy(h.data(), cnt, 4ull * V, cudaMemcpyDeviceToHost), "chunks");
+    std::vector<uint64_t> hs(V + 1, 0);
+    for (uint32_t v = 0; v < V; ++v) hs[v + 1] = hs[v] + h[v];
+    nchunks_ = hs[V];
+    check_cuda(cudaMemcpy(start, hs.data(), 8ull * (V + 1), cudaMemcpyHostToDevice), "chunks");
+    check_cuda(cudaMalloc(&chunks_, sizeof(uint2) * (nchunks_ ? nchunks_ : 1)), "chunks");
+    detail::k_fill_chunks<<<grid(V), 256>>>(in_off(), V, start, chunks_);
+    check_cuda(cudaDeviceSynchronize(), "chunks");
+    cudaFree(cnt);
+    cudaFree(start);
+    chunks_reversed_ = reversed_;
+  }
+
+  void compact(bitmap_t& actives, uint64_t* n, uint64_t* active_edges) {
+    const uint32_t V = view_.vertices;
+    if (!queue_) check_cuda(cudaMalloc(&queue_, 4ull * (V ? V : 1)), "queue");
+    if (!counters_) check_cuda(cudaMalloc(&counters_, 16), "counters");
+    check_cuda(cudaMemset(counters_, 0, 16), "counters");
+    const uint32_t* deg = reversed_ ? view_.in_degree : view_.out_degree;
+    detail::k_compact<<<grid(V), 256>>>(actives.data(), V, deg, queue_, counters_);
+    unsigned long long h[2];
+    check_cuda(cudaMemcpy(h, counters_, 16, cudaMemcpyDeviceToHost), "counters");
+    *n = h[0];
+    *active_edges = h[1];
+  }
+
+  template <typename MSG, typename R, typename SIG, typename SLOT>
+  R push_queue(SIG signal, SLOT slot, uint64_t n) {
+    R* res = result_buf<R>();
+    if (n) {
+      detail::k_push<MSG, R><<<grid(n), 256>>>(queue_, n, signal, slot, res);
+      check_cuda(cudaGetLastError(), "push launch");
+    }
+    return read_result<R>(res);
+  }
+
+  template <typename R>
+  R* result_buf() {
+    if (!result_) check_cuda(cudaMalloc(&result_, 16), "result");
+    check_cuda(cudaMemset(result_, 0, 16), "result");
+    return reinterpret_cast<R*>(result_);
+  }
+  template <typename R>
+  R read_result(R* res) {
+    R h{};
+    check_cuda(cudaMemcpy(&h, res, sizeof(R), cudaMemcpyDeviceToHost), "result");
+    return h;
+  }
+
+  plato_graph* g_;
+  dualmode_engine_opts_t opts_;
+  plato_graph_device_view view_{};
+  plato_graph_info info_{};
+  bool reversed_ = false, chunks_reversed_ = false, last_push_ = false;
+  uint2* chunks_ = nullptr;
+  uint64_t nchunks_ = 0;
+  vid_t* queue_ = nullptr;
+  unsigned long long* counters_ = nullptr;
+  void* result_ = nullptr;
+};
+
+}  // namespace plato_b200

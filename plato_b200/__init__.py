@@ -227,6 +227,29 @@ class Graph:
               "plato_personalized_pagerank")
         return out, RunStats.from_c(s)
 
+    def ppr_batch(self, seed_sets, max_iterations: int = 100, damping: float = 0.85,
+                  eps: float = 1e-6, topk: int = 0, k_tile: int = 0, ranks: bool = False):
+        """Batched multi-source PPR: one query per seed set (trustrank seed-set
+        semantics).  -> dict(iterations [K], ranks [K, V] or None,
+        topk_ids [K, topk], topk_vals [K, topk])."""
+        K = len(seed_sets)
+        off = np.zeros(K + 1, dtype=np.uint64)
+        off[1:] = np.cumsum([len(s) for s in seed_sets])
+        flat = _u32(np.concatenate([np.asarray(s, dtype=np.uint32) for s in seed_sets])
+                    if K else np.zeros(0, np.uint32))
+        V = self.vertices
+        out_r = np.empty((K, V), dtype=np.float32) if ranks else None
+        ids = np.empty((K, topk), dtype=np.uint32) if topk else None
+        vals = np.empty((K, topk), dtype=np.float32) if topk else None
+        its = np.empty(K, dtype=np.uint32)
+        o = _lib.PprBatchOpts(max_iterations, damping, eps, topk, k_tile)
+        check(self._lib.plato_ppr_batch(self.handle, K, _ptr(off), _ptr(flat), C.byref(o),
+                                        _ptr(out_r) if ranks else None,
+                                        _ptr(ids) if topk else None,
+                                        _ptr(vals) if topk else None, _ptr(its)),
+              "plato_ppr_batch")
+        return {"iterations": its, "ranks": out_r, "topk_ids": ids, "topk_vals": vals}
+
     def bfs(self, root: int, push_threshold: float = 0.05, parents: bool = True):
         """-> (levels uint32 [V] with PLATO_LEVEL_UNREACHED, parents or None, stats)."""
         V = self.vertices
@@ -268,3 +291,70 @@ def breadth_first_search(graph: Graph, opts: bfs_opts_t | None = None,
     eo = engine_opts or dualmode_engine_opts_t()
     _, _, st = graph.bfs(opts.root_, eo.push_threshold_, parents=False)
     return st.visited
+
+
+class PPRServer:
+    """Continuous-batching personalized PageRank server over a resident Graph.
+
+    submit() queues a seed set; step() admits queued requests into free slots
+    (bounded by ``hbm_budget_bytes``), runs one iteration over every live
+    query and retires the converged ones with their top-k; poll() returns
+    finished results."""
+
+    def __init__(self, graph: Graph, max_slots: int = 256, hbm_budget_bytes: int = 8 << 30,
+                 max_iterations: int = 200, damping: float = 0.85, eps: float = 1e-6,
+                 topk: int = 100):
+        self._lib = load()
+        self.graph = graph
+        self.topk = topk
+        o = _lib.ServerOpts(max_slots, hbm_budget_bytes, max_iterations, damping, eps, topk)
+        h = C.c_void_p()
+        check(self._lib.plato_server_create(graph.handle, C.byref(o), C.byref(h)),
+              "plato_server_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.plato_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, seeds) -> int:
+        s = _u32(seeds)
+        rid = C.c_uint64()
+        check(self._lib.plato_server_submit(self._h, _ptr(s), s.size, C.byref(rid)),
+              "plato_server_submit")
+        return int(rid.value)
+
+    def step(self) -> None:
+        check(self._lib.plato_server_step(self._h), "plato_server_step")
+
+    def poll(self):
+        """-> (request_id, topk_ids, topk_vals, iterations) or None."""
+        rid = C.c_uint64()
+        ids = np.empty(self.topk, dtype=np.uint32)
+        vals = np.empty(self.topk, dtype=np.float32)
+        it = C.c_uint32()
+        rc = self._lib.plato_server_poll(self._h, C.byref(rid), _ptr(ids), _ptr(vals), C.byref(it))
+        if rc == _lib.PLATO_ENOTFOUND:
+            return None
+        check(rc, "plato_server_poll")
+        return int(rid.value), ids, vals, int(it.value)
+
+    def stats(self):
+        live, queued = C.c_uint32(), C.c_uint32()
+        done = C.c_uint64()
+        check(self._lib.plato_server_stats(self._h, C.byref(live), C.byref(queued), C.byref(done)),
+              "plato_server_stats")
+        return {"live": int(live.value), "queued": int(queued.value), "completed": int(done.value)}

@@ -1,0 +1,349 @@
+// Batched multi-source personalized PageRank: one pull sweep serves many
+// queries (columns) at once.
+//
+// Semantics per column q (seed set S_q) follow algo::trustrank
+// (plato/algo/trustrank/trustrank.hpp:197-245) with explicit seeds:
+//   init      x = (1/|S_q|) / deg on seeds (1/|S_q| when deg == 0), 0 elsewhere
+//   epoch     y = sum over in-edges of x;  r = tele_q(v) + d * y,
+//             tele_q(v) = (1-d)/|S_q| on seeds, 0 elsewhere;
+//             x' = r / deg (deg > 0) or r; delta_q = sum |x' - x| * deg
+//   stop      after a non-final epoch with delta_q < eps, or at epoch
+//             max_iterations - 1, the next epoch is the final one and stores r
+//             (pagerank.hpp:118-140).
+//
+// Layout (HBM): the V x K state is stored tile-major, X[tile][v][kt], one
+// tile = kt consecutive columns, so one sweep over a tile touches a dense
+// V x kt block (kt*4 bytes per vertex, whole L2 sectors) and the vertex-row
+// gather of an edge is one coalesced kt-float load.  Each column tile is one
+// launch of k_batch_pull over the same merge-path tiles as the scalar pull
+// kernel; a group of GL lanes owns a run of merge items and each lane holds
+// VEC columns (kt = GL * VEC).  Column states live on the device, so a whole
+// iteration is a fixed launch sequence that is captured in a CUDA graph.
+#pragma once
+
+#include "graph.cuh"
+
+namespace plato_b200 {
+
+enum : uint8_t { COL_FREE = 0, COL_LIVE = 1, COL_FINAL = 2, COL_DONE = 3 };
+
+constexpr int kBatchTile = 4096;  // merge items per CTA (same tiles as the scalar pull)
+
+struct seed_index_view {
+  const uint32_t* off;   // [V+1] by internal vertex
+  const uint32_t* col;   // [S] global column
+  const float* tele;     // [S] (1-d)/|S_q|
+};
+
+struct batch_pass {
+  const uint32_t* trow;
+  const uint64_t* tedge;
+  uint32_t T;
+  uint32_t V;
+  uint32_t rows;         // partial rows per column tile: T + fixup blocks
+  const uint64_t* off;
+  const uint32_t* adj;
+  const uint32_t* deg;
+  const float* X;   // column tile ct at X + ct * V * kt: [V][kt]
+  float* Xn;
+  const uint8_t* state;  // [K] column states
+  seed_index_view seeds;
+  uint32_t col_base;     // global column of the tile's first column (set per tile)
+  float d;
+  float* tcarry;         // per column tile: [T][kt]
+  float* thead;          // per column tile: [T][kt]
+  double* partials;      // per column tile: [rows][kt]
+};
+
+// Pointers of column tile blockIdx.y (grids are (tiles, column tiles)).
+template <int KT>
+__device__ __forceinline__ batch_pass batch_tile_view(const batch_pass& p) {
+  batch_pass q = p;
+  const size_t ct = blockIdx.y;
+  q.X += ct * p.V * KT;
+  q.Xn += ct * p.V * KT;
+  q.state += ct * KT;
+  q.col_base = static_cast<uint32_t>(ct * KT);
+  q.tcarry += ct * p.T * KT;
+  q.thead += ct * p.T * KT;
+  q.partials += ct * p.rows * KT;
+  return q;
+}
+
+template <int VEC>
+__device__ __forceinline__ void ldvec(const float* p, float (&a)[VEC]) {
+  if constexpr (VEC == 1) {
+    a[0] = __ldg(p);
+  } else if constexpr (VEC == 2) {
+    const float2 t = __ldg(reinterpret_cast<const float2*>(p));
+    a[0] = t.x;
+    a[1] = t.y;
+  } else {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+    a[0] = t.x;
+    a[1] = t.y;
+    a[2] = t.z;
+    a[3] = t.w;
+  }
+}
+
+// Update of one vertex row for this lane's VEC columns.
+template <int GL, int VEC>
+__device__ __forceinline__ void batch_finalize(const batch_pass& p, uint32_t v,
+                                               const float (&y)[VEC], const uint8_t (&st)[VEC],
+                                               int lane_g, double (&dl)[VEC]) {
+  constexpr int KT = GL * VEC;
+  float tele[VEC];
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) tele[c] = 0.f;
+  const uint32_t s0 = p.seeds.off[v], s1 = p.seeds.off[v + 1];
+  for (uint32_t e = s0; e < s1; ++e) {
+    const uint32_t c = p.seeds.col[e] - p.col_base - static_cast<uint32_t>(lane_g * VEC);
+#pragma unroll
+    for (int k = 0; k < VEC; ++k)
+      if (c == static_cast<uint32_t>(k)) tele[k] += p.seeds.tele[e];
+  }
+  const uint32_t dg = p.deg[v];
+  const size_t base = static_cast<size_t>(v) * KT + lane_g * VEC;
+  float old[VEC];
+  ldvec<VEC>(p.X + base, old);
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) {
+    const float r = fmaf(p.d, y[c], tele[c]);
+    if (st[c] == COL_LIVE) {
+      float xv, dlt;
+      if (dg > 0) {
+        const float fd = static_cast<float>(dg);
+        xv = r / fd;
+        dlt = fabsf(xv - old[c]) * fd;
+      } else {
+        xv = r;
+        dlt = fabsf(xv - old[c]);
+      }
+      p.Xn[base + c] = xv;
+      dl[c] += static_cast<double>(dlt);
+    } else if (st[c] == COL_FINAL) {
+      p.Xn[base + c] = r;
+    }
+  }
+}
+
+// Merge-path search in shared memory: first coordinate of diagonal `diag`.
+__device__ __forceinline__ void merge_search(const uint32_t* s_rowend, int nrows, int nnz, int diag,
+                                             int& row, int& edge) {
+  int lo = max(diag - nnz, 0), hi = min(diag, nrows);
+  while (lo < hi) {
+    const int piv = (lo + hi) >> 1;
+    if (static_cast<int>(s_rowend[piv]) <= diag - piv - 1)
+      lo = piv + 1;
+    else
+      hi = piv;
+  }
+  row = lo;
+  edge = diag - lo;
+}
+
+template <int GL, int VEC>
+__global__ void __launch_bounds__(256) k_batch_pull(batch_pass p0) {
+  constexpr int KT = GL * VEC, NG = 256 / GL, TILE = kBatchTile, IPG = TILE / NG;
+  const batch_pass p = batch_tile_view<KT>(p0);
+  __shared__ uint32_t s_rowend[TILE];
+  __shared__ uint32_t s_src[TILE];
+  __shared__ uint32_t s_ckey[NG];
+  __shared__ float s_cval[NG * KT];
+  __shared__ double s_dl[NG * KT];
+
+  const int lane_g = threadIdx.x % GL, g = threadIdx.x / GL;
+  uint8_t st[VEC];
+  int mine = 0;
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) {
+    st[c] = p.state[lane_g * VEC + c];
+    mine |= (st[c] == COL_LIVE || st[c] == COL_FINAL);
+  }
+  if (!__syncthreads_or(mine)) return;  // every column of this tile is idle
+
+  const uint32_t t = blockIdx.x;
+  const uint32_t i0 = p.trow[t], i1 = p.trow[t + 1];
+  const uint64_t j0 = p.tedge[t], j1 = p.tedge[t + 1];
+  const int nrows = static_cast<int>(i1 - i0), nnz = static_cast<int>(j1 - j0);
+  const bool spans = p.off[i0] < j0;
+  for (int r = threadIdx.x; r < nrows; r += 256)
+    s_rowend[r] = static_cast<uint32_t>(p.off[i0 + r + 1] - j0);
+  for (int e = threadIdx.x; e < nnz; e += 256) s_src[e] = __ldg(p.adj + j0 + e);
+  __syncthreads();
+
+  const int total = nrows + nnz;
+  const int d0 = min(g * IPG, total), d1 = min(d0 + IPG, total);
+  int ra, ja, rb, jb;
+  merge_search(s_rowend, nrows, nnz, d0, ra, ja);
+  merge_search(s_rowend, nrows, nnz, d1, rb, jb);
+  const int head = ra;
+  bool head_done = false;
+  float acc[VEC], head_acc[VEC];
+  double dl[VEC];
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) {
+    acc[c] = 0.f;
+    head_acc[c] = 0.f;
+    dl[c] = 0.0;
+  }
+  const float* xl = p.X + lane_g * VEC;
+  int jj = ja;
+  for (int r = ra; r <= rb; ++r) {
+    const int e_end = (r < rb) ? static_cast<int>(s_rowend[r]) : jb;
+    for (; jj + 4 <= e_end; jj += 4) {
+      float a0[VEC], a1[VEC], a2[VEC], a3[VEC];
+      ldvec<VEC>(xl + static_cast<size_t>(s_src[jj]) * KT, a0);
+      ldvec<VEC>(xl + static_cast<size_t>(s_src[jj + 1]) * KT, a1);
+      ldvec<VEC>(xl + static_cast<size_t>(s_src[jj + 2]) * KT, a2);
+      ldvec<VEC>(xl + static_cast<size_t>(s_src[jj + 3]) * KT, a3);
+#pragma unroll
+      for (int c = 0; c < VEC; ++c) acc[c] += (a0[c] + a1[c]) + (a2[c] + a3[c]);
+    }
+    for (; jj < e_end; ++jj) {
+      float a0[VEC];
+      ldvec<VEC>(xl + static_cast<size_t>(s_src[jj]) * KT, a0);
+#pragma unroll
+      for (int c = 0; c < VEC; ++c) acc[c] += a0[c];
+    }
+    if (r < rb) {
+      if (r == head) {
+        head_done = true;
+#pragma unroll
+        for (int c = 0; c < VEC; ++c) head_acc[c] = acc[c];
+      } else {
+        batch_finalize<GL, VEC>(p, i0 + r, acc, st, lane_g, dl);
+      }
+#pragma unroll
+      for (int c = 0; c < VEC; ++c) acc[c] = 0.f;
+    }
+  }
+  if (lane_g == 0) s_ckey[g] = static_cast<uint32_t>(rb);
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) s_cval[g * KT + lane_g * VEC + c] = acc[c];
+  __syncthreads();
+
+  if (head_done) {
+    float y[VEC];
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) y[c] = head_acc[c];
+    for (int g2 = g - 1; g2 >= 0 && s_ckey[g2] == static_cast<uint32_t>(head); --g2) {
+#pragma unroll
+      for (int c = 0; c < VEC; ++c) y[c] += s_cval[g2 * KT + lane_g * VEC + c];
+    }
+    if (head == 0 && spans) {
+#pragma unroll
+      for (int c = 0; c < VEC; ++c) p.thead[static_cast<size_t>(t) * KT + lane_g * VEC + c] = y[c];
+    } else {
+      batch_finalize<GL, VEC>(p, i0 + head, y, st, lane_g, dl);
+    }
+  }
+  if (g == NG - 1) {
+    float y[VEC];
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) y[c] = 0.f;
+    for (int g2 = NG - 1; g2 >= 0 && s_ckey[g2] == static_cast<uint32_t>(nrows); --g2) {
+#pragma unroll
+      for (int c = 0; c < VEC; ++c) y[c] += s_cval[g2 * KT + lane_g * VEC + c];
+    }
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) p.tcarry[static_cast<size_t>(t) * KT + lane_g * VEC + c] = y[c];
+  }
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) s_dl[g * KT + lane_g * VEC + c] = dl[c];
+  __syncthreads();
+  for (int c = threadIdx.x; c < KT; c += 256) {
+    double s = 0.0;
+    for (int g2 = 0; g2 < NG; ++g2) s += s_dl[g2 * KT + c];
+    p.partials[static_cast<size_t>(t) * KT + c] = s;
+  }
+}
+
+// Rows split across CTAs: one group of GL lanes per tile.
+template <int GL, int VEC>
+__global__ void __launch_bounds__(256) k_batch_fixup(batch_pass p0) {
+  constexpr int KT = GL * VEC, NG = 256 / GL;
+  const batch_pass p = batch_tile_view<KT>(p0);
+  __shared__ double s_dl[NG * KT];
+  const int lane_g = threadIdx.x % GL, g = threadIdx.x / GL;
+  uint8_t st[VEC];
+  int mine = 0;
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) {
+    st[c] = p.state[lane_g * VEC + c];
+    mine |= (st[c] == COL_LIVE || st[c] == COL_FINAL);
+  }
+  if (!__syncthreads_or(mine)) return;
+  double dl[VEC];
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) dl[c] = 0.0;
+  const uint32_t t = blockIdx.x * NG + g;
+  if (t >= 1 && t < p.T) {
+    const uint32_t i0 = p.trow[t];
+    if (p.trow[t + 1] > i0 && p.off[i0] < p.tedge[t]) {
+      uint32_t tf = t - 1;
+      while (tf > 0 && p.trow[tf] == i0) --tf;
+      float y[VEC];
+#pragma unroll
+      for (int c = 0; c < VEC; ++c) y[c] = 0.f;
+      for (uint32_t u = tf; u < t; ++u) {
+#pragma unroll
+        for (int c = 0; c < VEC; ++c) y[c] += p.tcarry[static_cast<size_t>(u) * KT + lane_g * VEC + c];
+      }
+#pragma unroll
+      for (int c = 0; c < VEC; ++c) y[c] += p.thead[static_cast<size_t>(t) * KT + lane_g * VEC + c];
+      batch_finalize<GL, VEC>(p, i0, y, st, lane_g, dl);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) s_dl[g * KT + lane_g * VEC + c] = dl[c];
+  __syncthreads();
+  for (int c = threadIdx.x; c < KT; c += 256) {
+    double s = 0.0;
+    for (int g2 = 0; g2 < NG; ++g2) s += s_dl[g2 * KT + c];
+    p.partials[(static_cast<size_t>(p.T) + blockIdx.x) * KT + c] = s;
+  }
+}
+
+// delta[q] = sum over rows of the column tile's partials[row][c] in row order;
+// grid (kt, column tiles), q = blockIdx.y * kt + blockIdx.x.
+static __global__ void __launch_bounds__(256) k_batch_delta(const double* __restrict__ partials,
+                                                            uint32_t rows, uint32_t kt,
+                                                            const uint8_t* __restrict__ state,
+                                                            double* __restrict__ delta) {
+  __shared__ double s_red[32];
+  const uint32_t c = blockIdx.x;
+  const uint32_t q = blockIdx.y * kt + c;
+  if (state[q] != COL_LIVE) return;  // block-uniform
+  const double* pt = partials + static_cast<size_t>(blockIdx.y) * rows * kt;
+  const uint32_t per = (rows + 255) / 256;
+  const uint32_t b = threadIdx.x * per, e = min(rows, b + per);
+  double acc = 0.0;
+  for (uint32_t i = b; i < e; ++i) acc += pt[static_cast<size_t>(i) * kt + c];
+  acc = block_sum<256>(acc, s_red);
+  if (threadIdx.x == 0) delta[q] = acc;
+}
+
+// Column state machine after one iteration (see the header comment).
+static __global__ void k_batch_states(uint32_t K, uint8_t* state, uint32_t* iters, uint8_t* parity,
+                               const double* __restrict__ delta, uint32_t max_iterations,
+                               double eps, int written_parity, uint32_t* live_count,
+                               uint32_t* retired, uint32_t* retired_count) {
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < K; q += gridDim.x * blockDim.x) {
+    const uint8_t s = state[q];
+    if (s == COL_LIVE) {
+      const uint32_t it = ++iters[q];
+      if (it >= max_iterations - 1 || (eps > 0.0 && delta[q] < eps)) state[q] = COL_FINAL;
+      atomicAdd(live_count, 1u);
+    } else if (s == COL_FINAL) {
+      ++iters[q];
+      state[q] = COL_DONE;
+      parity[q] = static_cast<uint8_t>(written_parity);
+      const uint32_t slot = atomicAdd(retired_count, 1u);
+      retired[slot] = q;
+    }
+  }
+}
+
+}  // namespace plato_b200

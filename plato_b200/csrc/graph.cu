@@ -263,8 +263,12 @@ int create_impl(const plato_graph_info* info, const uint32_t* src, const uint32_
 
 }  // namespace
 
-int ensure_pull_tiles(plato_graph* g, uint32_t items, cudaStream_t st) {
-  if (g->pull_tiles.items == items && g->pull_tiles.count > 0) return PLATO_OK;
+int ensure_pull_tiles(plato_graph* g, uint32_t items, cudaStream_t st, const merge_tiles** out) {
+  auto it = g->tiles.find(items);
+  if (it != g->tiles.end()) {
+    if (out) *out = &it->second;
+    return PLATO_OK;
+  }
   const uint64_t total = static_cast<uint64_t>(g->info.vertices) + g->stored_edges;
   const uint64_t T = (total + items - 1) / items;
   if (T >= 0xFFFFFFFFull) return set_error(PLATO_EINVAL, "graph too large for the tile size");
@@ -277,7 +281,9 @@ int ensure_pull_tiles(plato_graph* g, uint32_t items, cudaStream_t st) {
                                                       g->stored_edges, items, mt.count, mt.row.p,
                                                       mt.edge.p);
   PLATO_LAUNCHED("k_merge_tiles");
-  g->pull_tiles = std::move(mt);
+  auto& slot = g->tiles[items];
+  slot = std::move(mt);
+  if (out) *out = &slot;
   return PLATO_OK;
 }
 
@@ -316,6 +322,19 @@ int lookup_internal(const plato_graph* g, uint32_t ext, uint32_t* internal, cuda
   PLATO_CUDA_TRY(cudaMemcpyAsync(internal, g->to_int.p + ext, sizeof(uint32_t),
                                  cudaMemcpyDeviceToHost, st));
   PLATO_CUDA_TRY(cudaStreamSynchronize(st));
+  return PLATO_OK;
+}
+
+int host_to_internal(plato_graph* g, const std::vector<uint32_t>** map, cudaStream_t st) {
+  *map = nullptr;
+  if (!g->relabeled) return PLATO_OK;
+  if (g->h_to_int.size() != g->info.vertices) {
+    g->h_to_int.resize(g->info.vertices);
+    PLATO_CUDA_TRY(cudaMemcpyAsync(g->h_to_int.data(), g->to_int.p,
+                                   g->info.vertices * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    PLATO_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  *map = &g->h_to_int;
   return PLATO_OK;
 }
 

@@ -2,8 +2,10 @@
 // vertex order, plus lazily built per-algorithm metadata and workspaces.
 #pragma once
 
+#include <map>
 #include <memory>
 #include <mutex>
+#include <vector>
 
 #include "common.cuh"
 
@@ -40,9 +42,11 @@ struct plato_graph {
   cudaStream_t stream = nullptr;  // stream of the host-buffer entry points
   std::mutex mu;                  // one algorithm call at a time per graph
 
-  plato_b200::merge_tiles pull_tiles;
+  std::map<uint32_t, plato_b200::merge_tiles> tiles;  // merge-path tiles by items per tile
   plato_b200::rank_workspace* rank_ws = nullptr;
   plato_b200::bfs_workspace* bfs_ws = nullptr;
+  std::vector<uint32_t> h_to_int;             // host copy of to_int (lazily)
+  std::map<uint32_t, uint32_t> batch_tuned;   // K bucket -> columns per tile (kt)
 
   ~plato_graph();
 };
@@ -50,7 +54,8 @@ struct plato_graph {
 namespace plato_b200 {
 
 // Builds (once) the merge-path tiles of the CSC for `items` per tile.
-int ensure_pull_tiles(plato_graph* g, uint32_t items, cudaStream_t st);
+int ensure_pull_tiles(plato_graph* g, uint32_t items, cudaStream_t st,
+                      const merge_tiles** out = nullptr);
 
 // out_ext[to_ext[i]] = in_int[i] (identity when the graph is not relabeled).
 int scatter_to_external_f32(const plato_graph* g, const float* in_int, float* out_ext,
@@ -64,5 +69,8 @@ inline uint32_t to_internal_host(const plato_graph* g, uint32_t v, const uint32_
 
 // Maps one caller id to the internal id (device lookup, synchronous).
 int lookup_internal(const plato_graph* g, uint32_t ext, uint32_t* internal, cudaStream_t st);
+
+// Host copy of to_int (caller id -> internal id), fetched once per graph.
+int host_to_internal(plato_graph* g, const std::vector<uint32_t>** map, cudaStream_t st);
 
 }  // namespace plato_b200

@@ -1,0 +1,495 @@
+// Batched multi-source PPR: host driver (batch_engine) and plato_ppr_batch.
+#include <algorithm>
+#include <new>
+#include <set>
+
+#include "batch.cuh"
+#include "batch_engine.hpp"
+#include "profile.cuh"
+#include "topk.cuh"
+
+namespace plato_b200 {
+namespace {
+
+constexpr int kKernelsPerIteration = 4;
+
+bool kt_supported(uint32_t kt) { return kt == 8 || kt == 16 || kt == 32 || kt == 64 || kt == 128; }
+int group_lanes(uint32_t kt) { return kt <= 32 ? static_cast<int>(kt) : 32; }
+
+template <int GL, int VEC>
+int launch_pass(const batch_pass& p, uint32_t T, uint32_t fix_blocks, uint32_t ntiles,
+                cudaStream_t st) {
+  k_batch_pull<GL, VEC><<<dim3(T, ntiles), 256, 0, st>>>(p);
+  PLATO_LAUNCHED("k_batch_pull");
+  k_batch_fixup<GL, VEC><<<dim3(fix_blocks, ntiles), 256, 0, st>>>(p);
+  PLATO_LAUNCHED("k_batch_fixup");
+  return PLATO_OK;
+}
+
+// X[tile(q)][v][q % kt] = 0 for the listed columns.
+__global__ void k_zero_columns(float* X, uint32_t V, uint32_t kt, const uint32_t* cols,
+                               uint32_t ncols) {
+  const uint64_t total = static_cast<uint64_t>(V) * ncols;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t q = cols[i / V];
+    const uint32_t v = static_cast<uint32_t>(i % V);
+    X[(static_cast<size_t>(q / kt) * V + v) * kt + q % kt] = 0.f;
+  }
+}
+
+// Seed initial values (trustrank.hpp:197-206): (1/|S|) / deg, or 1/|S| when deg == 0.
+__global__ void k_seed_init(float* X, uint32_t V, uint32_t kt, const uint32_t* sv,
+                            const uint32_t* sq, const float* init, uint32_t n,
+                            const uint32_t* __restrict__ deg) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t v = sv[i], q = sq[i];
+    const uint32_t dg = deg[v];
+    X[(static_cast<size_t>(q / kt) * V + v) * kt + q % kt] = dg > 0 ? init[i] / static_cast<float>(dg) : init[i];
+  }
+}
+
+__global__ void k_set_states(uint8_t* state, uint32_t* iters, const uint32_t* cols, uint32_t n,
+                             uint8_t value) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    state[cols[i]] = value;
+    iters[cols[i]] = 0;
+  }
+}
+
+// out[i][caller id] = rank of column cols[i] (from the buffer holding its result).
+__global__ void k_gather_columns(const float* X0, const float* X1, const uint8_t* parity,
+                                 uint32_t V, uint32_t kt, const uint32_t* cols, uint32_t ncols,
+                                 const uint32_t* to_ext, float* out) {
+  const uint64_t total = static_cast<uint64_t>(V) * ncols;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t ci = static_cast<uint32_t>(i / V), v = static_cast<uint32_t>(i % V);
+    const uint32_t q = cols[ci];
+    const float* X = parity[q] ? X1 : X0;
+    const float val = X[(static_cast<size_t>(q / kt) * V + v) * kt + q % kt];
+    out[static_cast<size_t>(ci) * V + (to_ext ? to_ext[v] : v)] = val;
+  }
+}
+
+template <typename T>
+int upload(dbuf<T>& d, const std::vector<T>& h, cudaStream_t st) {
+  PLATO_TRY(d.alloc(std::max<size_t>(h.size(), 1)));
+  if (!h.empty())
+    PLATO_CUDA_TRY(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  return PLATO_OK;
+}
+
+}  // namespace
+
+batch_engine::~batch_engine() {
+  for (auto& e : exec_)
+    if (e) cudaGraphExecDestroy(e);
+  if (h_counters_) cudaFreeHost(h_counters_);
+}
+
+int batch_engine::init(uint32_t K, uint32_t kt, uint32_t max_iterations, double damping,
+                       double eps, cudaStream_t st) {
+  if (K == 0) return set_error(PLATO_EINVAL, "batched ppr: no queries");
+  if (!kt_supported(kt)) return set_error(PLATO_EINVAL, "batched ppr: k_tile must be 8/16/32/64/128");
+  if (max_iterations == 0) return set_error(PLATO_EINVAL, "batched ppr: max_iterations must be >= 1");
+  if (!(damping >= 0.0 && damping <= 1.0)) return set_error(PLATO_EINVAL, "damping must be in [0, 1]");
+  st_ = st;
+  K_ = K;
+  kt_ = kt;
+  Kp_ = (K + kt - 1) / kt * kt;
+  ntiles_ = Kp_ / kt;
+  max_iterations_ = max_iterations;
+  damping_ = damping;
+  eps_ = eps;
+  const uint32_t V = g_->info.vertices;
+  const merge_tiles* mt = nullptr;
+  PLATO_TRY(ensure_pull_tiles(g_, kBatchTile, st_, &mt));
+  const uint32_t T = mt->count;
+  const uint32_t NG = 256 / group_lanes(kt);
+  rows_ = T + (T + NG - 1) / NG;
+  const size_t cells = static_cast<size_t>(Kp_) * V;
+  PLATO_TRY(X_[0].alloc(cells));
+  PLATO_TRY(X_[1].alloc(cells));
+  PLATO_TRY(state_.alloc(Kp_));
+  PLATO_TRY(parity_.alloc(Kp_));
+  PLATO_TRY(iters_.alloc(Kp_));
+  PLATO_TRY(delta_.alloc(Kp_));
+  PLATO_TRY(tcarry_.alloc(static_cast<size_t>(ntiles_) * T * kt));
+  PLATO_TRY(thead_.alloc(static_cast<size_t>(ntiles_) * T * kt));
+  PLATO_TRY(partials_.alloc(static_cast<size_t>(ntiles_) * rows_ * kt));
+  PLATO_TRY(seed_off_.alloc(static_cast<size_t>(V) + 1));
+  PLATO_TRY(seed_col_.alloc(static_cast<size_t>(Kp_) * 64));
+  PLATO_TRY(seed_tele_.alloc(static_cast<size_t>(Kp_) * 64));
+  PLATO_TRY(counters_.alloc(2));
+  PLATO_TRY(retired_.alloc(Kp_));
+  PLATO_CUDA_TRY(cudaMemsetAsync(state_.p, COL_FREE, Kp_, st_));
+  PLATO_CUDA_TRY(cudaMemsetAsync(parity_.p, 0, Kp_, st_));
+  PLATO_CUDA_TRY(cudaMemsetAsync(iters_.p, 0, Kp_ * sizeof(uint32_t), st_));
+  PLATO_CUDA_TRY(cudaMemsetAsync(seed_off_.p, 0, (static_cast<size_t>(V) + 1) * sizeof(uint32_t), st_));
+  if (!h_counters_)
+    PLATO_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&h_counters_), (2 + Kp_) * sizeof(uint32_t)));
+  col_seeds_.assign(Kp_, {});
+  cur_ = 0;
+  return capture();
+}
+
+int batch_engine::launch_iteration(int parity) {
+  const uint32_t V = g_->info.vertices;
+  const merge_tiles& mt = g_->tiles.at(kBatchTile);
+  batch_pass p{};
+  p.trow = mt.row.p;
+  p.tedge = mt.edge.p;
+  p.T = mt.count;
+  p.V = V;
+  p.rows = rows_;
+  p.off = g_->in_off.p;
+  p.adj = g_->in_adj.p;
+  p.deg = g_->out_deg.p;
+  p.X = X_[parity].p;
+  p.Xn = X_[parity ^ 1].p;
+  p.state = state_.p;
+  p.seeds = seed_index_view{seed_off_.p, seed_col_.p, seed_tele_.p};
+  p.col_base = 0;
+  p.d = static_cast<float>(damping_);
+  p.tcarry = tcarry_.p;
+  p.thead = thead_.p;
+  p.partials = partials_.p;
+  const uint32_t T = mt.count;
+  PLATO_CUDA_TRY(cudaMemsetAsync(counters_.p, 0, 2 * sizeof(uint32_t), st_));
+  const uint32_t fix_blocks = rows_ - T;
+  switch (kt_) {
+    case 8: PLATO_TRY((launch_pass<8, 1>(p, T, fix_blocks, ntiles_, st_))); break;
+    case 16: PLATO_TRY((launch_pass<16, 1>(p, T, fix_blocks, ntiles_, st_))); break;
+    case 32: PLATO_TRY((launch_pass<32, 1>(p, T, fix_blocks, ntiles_, st_))); break;
+    case 64: PLATO_TRY((launch_pass<32, 2>(p, T, fix_blocks, ntiles_, st_))); break;
+    default: PLATO_TRY((launch_pass<32, 4>(p, T, fix_blocks, ntiles_, st_))); break;
+  }
+  k_batch_delta<<<dim3(kt_, ntiles_), 256, 0, st_>>>(partials_.p, rows_, kt_, state_.p, delta_.p);
+  PLATO_LAUNCHED("k_batch_delta");
+  k_batch_states<<<grid_for(Kp_, 256, 64), 256, 0, st_>>>(
+      Kp_, state_.p, iters_.p, parity_.p, delta_.p, max_iterations_, eps_, parity ^ 1,
+      counters_.p, retired_.p, counters_.p + 1);
+  PLATO_LAUNCHED("k_batch_states");
+  PLATO_CUDA_TRY(cudaMemcpyAsync(h_counters_, counters_.p, 2 * sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, st_));
+  PLATO_CUDA_TRY(cudaMemcpyAsync(h_counters_ + 2, retired_.p, Kp_ * sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, st_));
+  return PLATO_OK;
+}
+
+int batch_engine::capture() {
+  for (int parity = 0; parity < 2; ++parity) {
+    if (exec_[parity]) {
+      cudaGraphExecDestroy(exec_[parity]);
+      exec_[parity] = nullptr;
+    }
+    cudaGraph_t graph = nullptr;
+    PLATO_CUDA_TRY(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+    const int s = launch_iteration(parity);
+    const cudaError_t e = cudaStreamEndCapture(st_, &graph);
+    if (s != PLATO_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return s;
+    }
+    PLATO_CUDA_TRY(e);
+    const cudaError_t ie = cudaGraphInstantiate(&exec_[parity], graph, 0);
+    cudaGraphDestroy(graph);
+    PLATO_CUDA_TRY(ie);
+  }
+  return PLATO_OK;
+}
+
+int batch_engine::rebuild_seed_index() {
+  const uint32_t V = g_->info.vertices;
+  struct ent {
+    uint32_t v, q;
+    float tele;
+  };
+  std::vector<ent> ents;
+  for (uint32_t q = 0; q < Kp_; ++q) {
+    const auto& s = col_seeds_[q];
+    if (s.empty()) continue;
+    const float tele = static_cast<float>((1.0 - damping_) / static_cast<double>(s.size()));
+    for (uint32_t v : s) ents.push_back({v, q, tele});
+  }
+  std::sort(ents.begin(), ents.end(), [](const ent& a, const ent& b) {
+    return a.v != b.v ? a.v < b.v : a.q < b.q;
+  });
+  std::vector<uint32_t> off(static_cast<size_t>(V) + 1, 0), col(ents.size());
+  std::vector<float> tele(ents.size());
+  for (size_t i = 0; i < ents.size(); ++i) {
+    off[ents[i].v + 1]++;
+    col[i] = ents[i].q;
+    tele[i] = ents[i].tele;
+  }
+  for (uint32_t v = 0; v < V; ++v) off[v + 1] += off[v];
+  bool recapture = false;
+  if (ents.size() > seed_col_.n) {
+    PLATO_TRY(seed_col_.alloc(ents.size() * 2));
+    PLATO_TRY(seed_tele_.alloc(ents.size() * 2));
+    recapture = true;
+  }
+  PLATO_CUDA_TRY(cudaMemcpyAsync(seed_off_.p, off.data(), off.size() * sizeof(uint32_t),
+                                 cudaMemcpyHostToDevice, st_));
+  if (!ents.empty()) {
+    PLATO_CUDA_TRY(cudaMemcpyAsync(seed_col_.p, col.data(), col.size() * sizeof(uint32_t),
+                                   cudaMemcpyHostToDevice, st_));
+    PLATO_CUDA_TRY(cudaMemcpyAsync(seed_tele_.p, tele.data(), tele.size() * sizeof(float),
+                                   cudaMemcpyHostToDevice, st_));
+  }
+  PLATO_CUDA_TRY(cudaStreamSynchronize(st_));  // host vectors go out of scope
+  if (recapture) PLATO_TRY(capture());
+  return PLATO_OK;
+}
+
+int batch_engine::admit(const std::vector<uint32_t>& cols,
+                        const std::vector<std::vector<uint32_t>>& seeds) {
+  const uint32_t V = g_->info.vertices;
+  if (cols.size() != seeds.size()) return set_error(PLATO_EINVAL, "admit: size mismatch");
+  if (cols.empty()) return PLATO_OK;
+  const std::vector<uint32_t>* to_int = nullptr;
+  PLATO_TRY(host_to_internal(g_, &to_int, st_));
+  std::vector<uint32_t> sv, sq;
+  std::vector<float> init;
+  for (size_t i = 0; i < cols.size(); ++i) {
+    const uint32_t q = cols[i];
+    if (q >= K_) return set_error(PLATO_EINVAL, "admit: column out of range");
+    std::set<uint32_t> uniq;
+    for (uint32_t v : seeds[i]) {
+      if (v >= V) return set_error(PLATO_EINVAL, "ppr: seed vertex out of range");
+      uniq.insert(to_int ? (*to_int)[v] : v);
+    }
+    if (uniq.empty()) return set_error(PLATO_EINVAL, "ppr: empty seed set");
+    col_seeds_[q].assign(uniq.begin(), uniq.end());
+    const float iv = static_cast<float>(1.0 / static_cast<double>(uniq.size()));
+    for (uint32_t v : uniq) {
+      sv.push_back(v);
+      sq.push_back(q);
+      init.push_back(iv);
+    }
+  }
+  dbuf<uint32_t> d_cols, d_sv, d_sq;
+  dbuf<float> d_init;
+  PLATO_TRY(upload(d_cols, cols, st_));
+  PLATO_TRY(upload(d_sv, sv, st_));
+  PLATO_TRY(upload(d_sq, sq, st_));
+  PLATO_TRY(upload(d_init, init, st_));
+  const uint32_t n = static_cast<uint32_t>(cols.size());
+  k_zero_columns<<<grid_for(static_cast<uint64_t>(V) * n, 256), 256, 0, st_>>>(X_[cur_].p, V, kt_,
+                                                                               d_cols.p, n);
+  PLATO_LAUNCHED("k_zero_columns");
+  k_seed_init<<<grid_for(sv.size(), 256), 256, 0, st_>>>(X_[cur_].p, V, kt_, d_sv.p, d_sq.p,
+                                                         d_init.p, static_cast<uint32_t>(sv.size()),
+                                                         g_->out_deg.p);
+  PLATO_LAUNCHED("k_seed_init");
+  k_set_states<<<grid_for(n, 256), 256, 0, st_>>>(state_.p, iters_.p, d_cols.p, n,
+                                                  max_iterations_ == 1 ? COL_FINAL : COL_LIVE);
+  PLATO_LAUNCHED("k_set_states");
+  return rebuild_seed_index();  // synchronises before the temporaries go
+}
+
+int batch_engine::step(uint32_t* live, std::vector<uint32_t>* retired) {
+  {
+    prof_scope ps("batch_iteration", st_);
+    PLATO_CUDA_TRY(cudaGraphLaunch(exec_[cur_], st_));
+  }
+  count_launch(kKernelsPerIteration);
+  PLATO_CUDA_TRY(cudaStreamSynchronize(st_));
+  cur_ ^= 1;
+  *live = h_counters_[0];
+  const uint32_t nret = std::min(h_counters_[1], Kp_);
+  if (retired) {
+    retired->assign(h_counters_ + 2, h_counters_ + 2 + nret);
+    std::sort(retired->begin(), retired->end());
+  }
+  for (uint32_t i = 0; i < nret; ++i) col_seeds_[h_counters_[2 + i]].clear();
+  return PLATO_OK;
+}
+
+int batch_engine::release(const std::vector<uint32_t>& cols) {
+  if (cols.empty()) return PLATO_OK;
+  dbuf<uint32_t> d_cols;
+  PLATO_TRY(upload(d_cols, cols, st_));
+  const uint32_t n = static_cast<uint32_t>(cols.size());
+  k_set_states<<<grid_for(n, 256), 256, 0, st_>>>(state_.p, iters_.p, d_cols.p, n, COL_FREE);
+  PLATO_LAUNCHED("k_set_states");
+  for (uint32_t q : cols) col_seeds_[q].clear();
+  PLATO_CUDA_TRY(cudaStreamSynchronize(st_));
+  return PLATO_OK;
+}
+
+int batch_engine::iterations(std::vector<uint32_t>* out) {
+  out->resize(Kp_);
+  PLATO_CUDA_TRY(cudaMemcpyAsync(out->data(), iters_.p, Kp_ * sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, st_));
+  PLATO_CUDA_TRY(cudaStreamSynchronize(st_));
+  return PLATO_OK;
+}
+
+int batch_engine::ranks(const std::vector<uint32_t>& cols, float* out) {
+  const uint32_t V = g_->info.vertices;
+  const uint32_t chunk = std::max<uint32_t>(1, std::min<uint32_t>(64, static_cast<uint32_t>(cols.size())));
+  dbuf<float> d_out;
+  dbuf<uint32_t> d_cols;
+  PLATO_TRY(d_out.alloc(static_cast<size_t>(chunk) * V));
+  for (size_t c0 = 0; c0 < cols.size(); c0 += chunk) {
+    const uint32_t n = static_cast<uint32_t>(std::min<size_t>(chunk, cols.size() - c0));
+    std::vector<uint32_t> part(cols.begin() + c0, cols.begin() + c0 + n);
+    PLATO_TRY(upload(d_cols, part, st_));
+    k_gather_columns<<<grid_for(static_cast<uint64_t>(V) * n, 256), 256, 0, st_>>>(
+        X_[0].p, X_[1].p, parity_.p, V, kt_, d_cols.p, n, g_->relabeled ? g_->to_ext.p : nullptr,
+        d_out.p);
+    PLATO_LAUNCHED("k_gather_columns");
+    PLATO_CUDA_TRY(cudaMemcpyAsync(out + c0 * V, d_out.p, static_cast<size_t>(n) * V * sizeof(float),
+                                   cudaMemcpyDeviceToHost, st_));
+    PLATO_CUDA_TRY(cudaStreamSynchronize(st_));
+  }
+  return PLATO_OK;
+}
+
+int batch_engine::topk(const std::vector<uint32_t>& cols, uint32_t k, uint32_t* ids, float* vals) {
+  if (cols.empty() || k == 0) return PLATO_OK;
+  if (k > kTopkMax) return set_error(PLATO_EINVAL, "topk must be <= 1024");
+  const uint32_t n = static_cast<uint32_t>(cols.size());
+  dbuf<uint32_t> d_cols, hist, d_ids, undone;
+  dbuf<topk_col> st;
+  dbuf<unsigned long long> cand;
+  dbuf<float> d_vals;
+  PLATO_TRY(upload(d_cols, cols, st_));
+  PLATO_TRY(st.alloc(n));
+  PLATO_TRY(hist.alloc(static_cast<size_t>(n) * 256));
+  PLATO_TRY(cand.alloc(static_cast<size_t>(n) * kCandCap));
+  PLATO_TRY(d_ids.alloc(static_cast<size_t>(n) * k));
+  PLATO_TRY(d_vals.alloc(static_cast<size_t>(n) * k));
+  PLATO_TRY(undone.alloc(1));
+  PLATO_CUDA_TRY(cudaMemsetAsync(hist.p, 0, static_cast<size_t>(n) * 256 * sizeof(uint32_t), st_));
+  topk_job j{};
+  j.buf[0] = X_[0].p;
+  j.buf[1] = X_[1].p;
+  j.parity = parity_.p;
+  j.cols = d_cols.p;
+  j.n = n;
+  j.V = g_->info.vertices;
+  j.kt = kt_;
+  j.to_ext = g_->relabeled ? g_->to_ext.p : nullptr;
+  j.st = st.p;
+  j.hist = hist.p;
+  j.cand = cand.p;
+  k_topk_init<<<grid_for(n, 256), 256, 0, st_>>>(j, k);
+  PLATO_LAUNCHED("k_topk_init");
+  const unsigned blocks = 148 * 4;
+  for (int pass = 0; pass < 8; ++pass) {
+    for (uint32_t c0 = 0; c0 < n; c0 += 32) {
+      k_topk_hist<<<blocks, 256, 0, st_>>>(j, c0);
+      PLATO_LAUNCHED("k_topk_hist");
+    }
+    PLATO_CUDA_TRY(cudaMemsetAsync(undone.p, 0, sizeof(uint32_t), st_));
+    k_topk_pick<<<grid_for(n, 256), 256, 0, st_>>>(j, k, undone.p);
+    PLATO_LAUNCHED("k_topk_pick");
+    uint32_t h_undone = 0;
+    PLATO_CUDA_TRY(cudaMemcpyAsync(&h_undone, undone.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st_));
+    PLATO_CUDA_TRY(cudaStreamSynchronize(st_));
+    if (h_undone == 0) break;
+  }
+  for (uint32_t c0 = 0; c0 < n; c0 += 32) {
+    k_topk_collect<<<blocks, 256, 0, st_>>>(j, c0);
+    PLATO_LAUNCHED("k_topk_collect");
+  }
+  k_topk_sort<<<n, 1024, 0, st_>>>(j, k, d_ids.p, d_vals.p);
+  PLATO_LAUNCHED("k_topk_sort");
+  PLATO_CUDA_TRY(cudaMemcpyAsync(ids, d_ids.p, static_cast<size_t>(n) * k * sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, st_));
+  PLATO_CUDA_TRY(cudaMemcpyAsync(vals, d_vals.p, static_cast<size_t>(n) * k * sizeof(float),
+                                 cudaMemcpyDeviceToHost, st_));
+  PLATO_CUDA_TRY(cudaStreamSynchronize(st_));
+  return PLATO_OK;
+}
+
+int batch_autotune(plato_graph* g, uint32_t K, cudaStream_t st, uint32_t* kt_out) {
+  uint32_t bucket = 8;
+  while (bucket < K && bucket < 128) bucket <<= 1;
+  auto it = g->batch_tuned.find(bucket);
+  if (it != g->batch_tuned.end()) {
+    *kt_out = it->second;
+    return PLATO_OK;
+  }
+  const uint32_t cands[] = {8, 16, 32, 64, 128};
+  double best = 1e300;
+  uint32_t best_kt = 32;
+  cudaEvent_t e0, e1;
+  PLATO_CUDA_TRY(cudaEventCreate(&e0));
+  PLATO_CUDA_TRY(cudaEventCreate(&e1));
+  for (uint32_t kt : cands) {
+    if (kt > bucket) break;
+    batch_engine eng(g);
+    PLATO_TRY(eng.init(kt, kt, 1u << 30, 0.85, 0.0, st));
+    std::vector<uint32_t> cols(kt);
+    std::vector<std::vector<uint32_t>> seeds(kt, std::vector<uint32_t>{0});
+    for (uint32_t q = 0; q < kt; ++q) cols[q] = q;
+    PLATO_TRY(eng.admit(cols, seeds));
+    uint32_t live = 0;
+    PLATO_TRY(eng.step(&live, nullptr));
+    PLATO_CUDA_TRY(cudaEventRecord(e0, st));
+    const int reps = 3;
+    for (int r = 0; r < reps; ++r) PLATO_TRY(eng.step(&live, nullptr));
+    PLATO_CUDA_TRY(cudaEventRecord(e1, st));
+    PLATO_CUDA_TRY(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    PLATO_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    // cost of a whole K-column iteration with this tile width
+    const double tiles = static_cast<double>((K + kt - 1) / kt);
+    const double cost = ms / reps * tiles;
+    if (cost < best) {
+      best = cost;
+      best_kt = kt;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  g->batch_tuned[bucket] = best_kt;
+  *kt_out = best_kt;
+  return PLATO_OK;
+}
+
+}  // namespace plato_b200
+
+using namespace plato_b200;
+
+extern "C" int plato_ppr_batch(plato_graph* g, uint32_t K, const uint64_t* seed_offsets,
+                               const plato_vid_t* seeds, const plato_ppr_batch_opts* opts,
+                               float* ranks, plato_vid_t* topk_ids, float* topk_vals,
+                               uint32_t* iterations) {
+  if (!g || !seed_offsets || !seeds || !opts)
+    return set_error(PLATO_EINVAL, "plato_ppr_batch: null argument");
+  if (K == 0) return set_error(PLATO_EINVAL, "plato_ppr_batch: K must be >= 1");
+  if (opts->topk > kTopkMax) return set_error(PLATO_EINVAL, "plato_ppr_batch: topk must be <= 1024");
+  if (opts->topk && (!topk_ids || !topk_vals))
+    return set_error(PLATO_EINVAL, "plato_ppr_batch: topk output buffers missing");
+  std::vector<std::vector<uint32_t>> sets(K);
+  std::vector<uint32_t> cols(K);
+  for (uint32_t q = 0; q < K; ++q) {
+    if (seed_offsets[q + 1] < seed_offsets[q])
+      return set_error(PLATO_EINVAL, "plato_ppr_batch: seed_offsets must be non-decreasing");
+    sets[q].assign(seeds + seed_offsets[q], seeds + seed_offsets[q + 1]);
+    cols[q] = q;
+  }
+  std::lock_guard<std::mutex> lock(g->mu);
+  PLATO_CUDA_TRY(cudaSetDevice(g->device));
+  cudaStream_t st = g->stream;
+  uint32_t kt = opts->k_tile;
+  if (kt == 0) PLATO_TRY(batch_autotune(g, K, st, &kt));
+  batch_engine eng(g);
+  PLATO_TRY(eng.init(K, kt, opts->max_iterations, opts->damping, opts->eps, st));
+  PLATO_TRY(eng.admit(cols, sets));
+  uint32_t live = K;
+  while (live > 0) PLATO_TRY(eng.step(&live, nullptr));
+  if (iterations) {
+    std::vector<uint32_t> it;
+    PLATO_TRY(eng.iterations(&it));
+    std::copy(it.begin(), it.begin() + K, iterations);
+  }
+  if (opts->topk) PLATO_TRY(eng.topk(cols, opts->topk, topk_ids, topk_vals));
+  if (ranks) PLATO_TRY(eng.ranks(cols, ranks));
+  return PLATO_OK;
+}

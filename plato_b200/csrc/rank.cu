@@ -15,6 +15,7 @@
 #include "graph.cuh"
 #include "profile.cuh"
 #include "pull_merge.cuh"
+#include "pull_warp.cuh"
 #include "push.cuh"
 
 namespace plato_b200 {
@@ -25,6 +26,8 @@ struct rank_workspace {
   dbuf<float> carry, head;
   dbuf<double> partials;
   dbuf<double> delta;
+  uint32_t sms = 0;           // CTAs of the persistent pull kernel
+  uint32_t hub_cap = 0;       // ranks the pull kernel can stage in shared memory
   double* h_delta = nullptr;  // pinned
   push_frontier frontier;
   ~rank_workspace() {
@@ -36,9 +39,33 @@ void destroy_rank_workspace(rank_workspace* ws) { delete ws; }
 
 namespace {
 
-constexpr int kNT = 256;
-constexpr int kIPT = 16;
-using cfg = pull_merge_cfg<kNT, kIPT>;
+#ifndef PLATO_PULL_IPT
+#define PLATO_PULL_IPT 7
+#endif
+constexpr int kIPT = PLATO_PULL_IPT;  // merge items per lane (odd: spreads lanes over banks)
+using cfg = pull_warp_cfg<kIPT>;
+
+// Opts the kernel into the largest dynamic shared memory the device allows
+// next to its static shared memory; returns the hub capacity (floats) that fits.
+template <class Tele>
+int set_pull_smem_attr(int device, uint32_t* hub_cap) {
+  static uint32_t cap = 0;
+  if (cap == 0) {
+    int optin = 0;
+    PLATO_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    cudaFuncAttributes fa{};
+    PLATO_CUDA_TRY(cudaFuncGetAttributes(&fa, k_pull_warp<kIPT, rank_update<Tele>>));
+    const size_t dyn = static_cast<size_t>(optin) - fa.sharedSizeBytes;
+    if (dyn <= cfg::kSlices + 64)
+      return set_error(PLATO_ECUDA, "pull kernel: not enough shared memory on this device");
+    PLATO_CUDA_TRY(cudaFuncSetAttribute(k_pull_warp<kIPT, rank_update<Tele>>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(dyn)));
+    cap = static_cast<uint32_t>((dyn - cfg::kSlices - 16) / 4 / 32 * 32);
+  }
+  *hub_cap = cap;
+  return PLATO_OK;
+}
 
 int ensure_ws(plato_graph* g, cudaStream_t st) {
   if (!g->rank_ws) {
@@ -47,27 +74,25 @@ int ensure_ws(plato_graph* g, cudaStream_t st) {
   }
   rank_workspace* ws = g->rank_ws;
   const uint32_t V = g->info.vertices;
-  PLATO_TRY(ensure_pull_tiles(g, cfg::kTile, st));
-  const uint32_t T = g->pull_tiles.count;
+  PLATO_TRY(ensure_pull_tiles(g, cfg::kItems, st));
+  if (ws->sms == 0) {
+    int sms = 0;
+    PLATO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
+    ws->sms = static_cast<uint32_t>(sms);
+  }
+  const uint32_t W = ws->sms * cfg::kWarps;
   PLATO_TRY(ws->x[0].alloc(V));
   PLATO_TRY(ws->x[1].alloc(V));
-  PLATO_TRY(ws->carry.alloc(T));
-  PLATO_TRY(ws->head.alloc(T));
-  const uint32_t fix_blocks = (T + 255) / 256;
-  // pull epochs use T + fix_blocks partials, dense (push) epochs up to 148 * 8
-  PLATO_TRY(ws->partials.alloc(std::max<size_t>(static_cast<size_t>(T) + fix_blocks + 1, 148 * 8)));
+  PLATO_TRY(ws->carry.alloc(W));
+  PLATO_TRY(ws->head.alloc(W));
+  // pull epochs: one partial per CTA + one per fixup block; dense epochs up to 148 * 8
+  PLATO_TRY(ws->partials.alloc(std::max<size_t>(ws->sms + (W + 255) / 256 + 1, 148 * 8)));
   PLATO_TRY(ws->delta.alloc(1));
   if (!ws->h_delta) PLATO_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&ws->h_delta), sizeof(double)));
-  static bool attr_set = false;
-  if (!attr_set) {
-    PLATO_CUDA_TRY(cudaFuncSetAttribute(k_pull_merge<kNT, kIPT, rank_update<teleport_uniform>>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(cfg::kSmem)));
-    PLATO_CUDA_TRY(cudaFuncSetAttribute(k_pull_merge<kNT, kIPT, rank_update<teleport_single>>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(cfg::kSmem)));
-    attr_set = true;
-  }
+  uint32_t cap_a = 0, cap_b = 0;
+  PLATO_TRY(set_pull_smem_attr<teleport_uniform>(g->device, &cap_a));
+  PLATO_TRY(set_pull_smem_attr<teleport_single>(g->device, &cap_b));
+  ws->hub_cap = std::min(cap_a, cap_b);
   return PLATO_OK;
 }
 
@@ -93,34 +118,35 @@ __global__ void k_init_single(const uint32_t* __restrict__ deg, uint32_t V, uint
   }
 }
 
-// One pull epoch: merge tiles + cross-tile fixup; partial deltas to ws->partials.
+// One pull epoch: persistent warp-tile gather + cross-range fixup; partial
+// deltas to ws->partials (one per CTA, then one per fixup block).
 template <class Tele>
 int pull_epoch(plato_graph* g, const float* x, float* xn, Tele tele, float d, bool final_epoch,
                cudaStream_t st) {
   rank_workspace* ws = g->rank_ws;
-  const merge_tiles& mt = g->pull_tiles;
+  const merge_tiles& mt = g->tiles.at(cfg::kItems);
   rank_update<Tele> upd{x, xn, g->out_deg.p, tele, d, final_epoch ? 1 : 0};
+  const uint32_t H = std::min<uint32_t>(g->info.vertices, ws->hub_cap);
+  pull_warp_args a{mt.row.p, mt.edge.p, mt.count, g->stored_edges, g->in_off.p, g->in_adj.p,
+                   x, H, ws->carry.p, ws->head.p, ws->partials.p};
   {
-    prof_scope ps("k_pull_merge", st);
-    k_pull_merge<kNT, kIPT, rank_update<Tele>><<<mt.count, kNT, cfg::kSmem, st>>>(
-        mt.row.p, mt.edge.p, g->in_off.p, g->in_adj.p, x, upd, ws->carry.p, ws->head.p,
-        ws->partials.p);
-    PLATO_LAUNCHED("k_pull_merge");
+    prof_scope ps("k_pull_warp", st);
+    k_pull_warp<kIPT, rank_update<Tele>><<<ws->sms, 1024, cfg::smem_bytes(H), st>>>(a, upd);
+    PLATO_LAUNCHED("k_pull_warp");
   }
-  const uint32_t fix_blocks = (mt.count + 255) / 256;
+  const uint32_t W = ws->sms * cfg::kWarps;
+  a.partials = ws->partials.p + ws->sms;
   {
-    prof_scope ps("k_pull_fixup", st);
-    k_pull_fixup<rank_update<Tele>><<<fix_blocks, 256, 0, st>>>(
-        mt.row.p, mt.edge.p, g->in_off.p, mt.count, upd, ws->carry.p, ws->head.p,
-        ws->partials.p + mt.count);
-    PLATO_LAUNCHED("k_pull_fixup");
+    prof_scope ps("k_pull_warp_fixup", st);
+    k_pull_warp_fixup<rank_update<Tele>><<<(W + 255) / 256, 256, 0, st>>>(a, W, upd);
+    PLATO_LAUNCHED("k_pull_warp_fixup");
   }
   return PLATO_OK;
 }
 
 int partial_count(const plato_graph* g) {
-  const uint32_t T = g->pull_tiles.count;
-  return static_cast<int>(T + (T + 255) / 256);
+  const uint32_t W = g->rank_ws->sms * cfg::kWarps;
+  return static_cast<int>(g->rank_ws->sms + (W + 255) / 256);
 }
 
 // Reads back the epoch's delta (sum of the partials).  Synchronises `st`.
