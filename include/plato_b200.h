@@ -46,7 +46,7 @@ extern "C" {
 #define PLATO_LEVEL_UNREACHED 0xFFFFFFFFu
 
 /* graph creation flags */
-#define PLATO_GRAPH_RELABEL 0x1u /* renumber vertices by descending out-degree inside the engine */
+#define PLATO_GRAPH_RELABEL 0x1u /* renumber vertices by descending in-degree inside the engine */
 
 /* personalized pagerank modes */
 #define PLATO_PPR_PULL      0 /* pull-only engine: personalized_pagerank.hpp:40-134     */
@@ -161,6 +161,11 @@ int plato_pagerank(plato_graph* g, const plato_pagerank_opts* opts, float* ranks
  * dual-mode (:137-275) by `mode`.  ranks: host [V]. */
 int plato_personalized_pagerank(plato_graph* g, const plato_ppr_opts* opts, int mode,
                                 float* ranks, plato_run_stats* stats);
+/* algo::trustrank (plato/algo/trustrank/trustrank.hpp:163-259) with the seed
+ * set given instead of selected: one seed-set PPR query on the pull engine
+ * (init 1/|S| on seeds, teleport (1-d)/|S| on seeds; opts->src is ignored). */
+int plato_seedset_ppr(plato_graph* g, const plato_vid_t* seeds, uint32_t n,
+                      const plato_ppr_opts* opts, float* ranks, plato_run_stats* stats);
 /* algo::breadth_first_search (plato/algo/bfs/bfs.hpp:55-155) with the engine's
  * push/pull switch (dualmode.hpp:245-297).  levels/parents: host [V] or NULL. */
 int plato_bfs(plato_graph* g, const plato_bfs_opts* opts, const plato_dualmode_opts* engine_opts,

@@ -227,6 +227,16 @@ class Graph:
               "plato_personalized_pagerank")
         return out, RunStats.from_c(s)
 
+    def seedset_ppr(self, seeds, iteration: int = 100, damping: float = 0.85, eps: float = 0.0):
+        """One seed-set PPR query on the pull engine (trustrank with explicit seeds)."""
+        s = _u32(seeds)
+        out = np.empty(self.vertices, dtype=np.float32)
+        o = _lib.PprOpts(iteration, damping, 0, eps)
+        st = _lib.RunStats()
+        check(self._lib.plato_seedset_ppr(self.handle, _ptr(s), s.size, C.byref(o), _ptr(out),
+                                          C.byref(st)), "plato_seedset_ppr")
+        return out, RunStats.from_c(st)
+
     def ppr_batch(self, seed_sets, max_iterations: int = 100, damping: float = 0.85,
                   eps: float = 1e-6, topk: int = 0, k_tile: int = 0, ranks: bool = False):
         """Batched multi-source PPR: one query per seed set (trustrank seed-set

@@ -94,6 +94,7 @@ SIGNATURES = {
     "plato_pagerank": (C.c_int, [P, C.POINTER(PagerankOpts), P, C.POINTER(RunStats)]),
     "plato_personalized_pagerank": (C.c_int, [P, C.POINTER(PprOpts), C.c_int, P, C.POINTER(RunStats)]),
     "plato_bfs": (C.c_int, [P, C.POINTER(BfsOpts), C.POINTER(DualmodeOpts), P, P, C.POINTER(RunStats)]),
+    "plato_seedset_ppr": (C.c_int, [P, P, C.c_uint32, C.POINTER(PprOpts), P, C.POINTER(RunStats)]),
     "plato_pagerank_device": (C.c_int, [P, C.POINTER(PagerankOpts), P, P, C.POINTER(RunStats)]),
     "plato_ppr_batch": (C.c_int, [P, C.c_uint32, P, P, C.POINTER(PprBatchOpts), P, P, P, P]),
     "plato_server_create": (C.c_int, [P, C.POINTER(ServerOpts), C.POINTER(P)]),

@@ -10,8 +10,10 @@
 // generate_dense_out_degrees_fg does (structure.hpp:291-346).
 //
 // With PLATO_GRAPH_RELABEL the engine renumbers vertices by descending
-// out-degree (ties by caller id) so the most-gathered rank values share cache
-// lines; to_int/to_ext map between the numberings.  Adjacency lists are sorted
+// in-degree (ties by caller id): CSC columns then form contiguous degree
+// bins for the pull kernels, and since in- and out-degree go together in
+// power-law graphs the most-gathered rank values share cache lines at the
+// front of the rank vector; to_int/to_ext map between the numberings.  Adjacency lists are sorted
 // ascending, so the graph is a pure function of the edge multiset.
 #include <cub/cub.cuh>
 
@@ -238,7 +240,7 @@ int create_impl(const plato_graph_info* info, const uint32_t* src, const uint32_
     dbuf<uint64_t> ka, kb;
     PLATO_TRY(ka.alloc(V));
     PLATO_TRY(kb.alloc(V));
-    k_relabel_keys<<<grid_for(V, 256), 256, 0, st>>>(deg_out_ext.p, V, ka.p);
+    k_relabel_keys<<<grid_for(V, 256), 256, 0, st>>>(deg_in_ext.p, V, ka.p);
     PLATO_LAUNCHED("k_relabel_keys");
     uint64_t* sorted = nullptr;
     PLATO_TRY(radix_sort(ka.p, kb.p, V, 64, tmp, st, &sorted));

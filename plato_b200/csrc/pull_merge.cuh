@@ -32,6 +32,14 @@ struct teleport_single {  // personalized_pagerank.hpp:105,113: (v == src ? 1-d 
   __device__ __forceinline__ float operator()(uint32_t v) const { return v == src ? val : 0.f; }
 };
 
+struct teleport_seeds {  // trustrank.hpp:226-245: (seed ? (1-d)/|S| : 0)
+  const uint32_t* bits;  // seed bitmap, 32-bit words
+  float val;
+  __device__ __forceinline__ float operator()(uint32_t v) const {
+    return ((bits[v >> 5] >> (v & 31)) & 1u) ? val : 0.f;
+  }
+};
+
 template <class Teleport>
 struct rank_update {
   const float* __restrict__ x;    // current state

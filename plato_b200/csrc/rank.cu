@@ -15,10 +15,22 @@
 #include "graph.cuh"
 #include "profile.cuh"
 #include "pull_merge.cuh"
+#include "pull_binned.cuh"
 #include "pull_warp.cuh"
 #include "push.cuh"
 
 namespace plato_b200 {
+
+// Degree-bin plan of a relabelled graph (see pull_binned.cuh).
+struct pull_plan {
+  bool valid = false;
+  uint32_t n_long = 0, n_mid = 0, n_items = 0, n_hubs = 0;
+  uint32_t blocks_long = 0, blocks_hubs = 0, blocks_mid = 0, blocks_short = 0;
+  dbuf<uint2> items;
+  dbuf<uint32_t> hub_rows, hub_item0, hub_pieces;
+  dbuf<float> piece_sum;
+  uint32_t partials() const { return blocks_long + blocks_hubs + blocks_mid + blocks_short; }
+};
 
 struct rank_workspace {
   dbuf<float> x[2];
@@ -28,6 +40,9 @@ struct rank_workspace {
   dbuf<double> delta;
   uint32_t sms = 0;           // CTAs of the persistent pull kernel
   uint32_t hub_cap = 0;       // ranks the pull kernel can stage in shared memory
+  bool plan_built = false;
+  pull_plan plan;
+  dbuf<uint32_t> seed_bits, seed_list;  // seed-set PPR
   double* h_delta = nullptr;  // pinned
   push_frontier frontier;
   ~rank_workspace() {
@@ -67,6 +82,57 @@ int set_pull_smem_attr(int device, uint32_t* hub_cap) {
   return PLATO_OK;
 }
 
+// Builds the degree-bin plan when the internal order sorts columns by
+// descending in-degree (relabelled graphs); otherwise plan.valid stays false
+// and the merge-path kernel handles the pull.
+int build_plan(plato_graph* g, pull_plan& pl, cudaStream_t st) {
+  const uint32_t V = g->info.vertices;
+  if (!g->relabeled) return PLATO_OK;
+  std::vector<uint32_t> deg(V);
+  PLATO_CUDA_TRY(cudaMemcpyAsync(deg.data(), g->in_deg.p, V * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  PLATO_CUDA_TRY(cudaStreamSynchronize(st));
+  for (uint32_t v = 1; v < V; ++v)
+    if (deg[v] > deg[v - 1]) return PLATO_OK;  // not sorted: keep the merge-path kernel
+  uint32_t n_long = 0, n_mid = 0;
+  while (n_long < V && deg[n_long] > kMidMax) ++n_long;
+  while (n_long + n_mid < V && deg[n_long + n_mid] > kShortMax) ++n_mid;
+  std::vector<uint2> items;
+  std::vector<uint32_t> hr, hi0, hp;
+  for (uint32_t r = 0; r < n_long; ++r) {
+    const uint32_t pieces = (deg[r] + kLongPiece - 1) / kLongPiece;
+    if (pieces > 1) {
+      hr.push_back(r);
+      hi0.push_back(static_cast<uint32_t>(items.size()));
+      hp.push_back(pieces);
+    }
+    for (uint32_t k = 0; k < pieces; ++k) items.push_back(make_uint2(r, k));
+  }
+  pl.n_long = n_long;
+  pl.n_mid = n_mid;
+  pl.n_items = static_cast<uint32_t>(items.size());
+  pl.n_hubs = static_cast<uint32_t>(hr.size());
+  PLATO_TRY(pl.items.alloc(std::max<size_t>(items.size(), 1)));
+  PLATO_TRY(pl.piece_sum.alloc(std::max<size_t>(items.size(), 1)));
+  PLATO_TRY(pl.hub_rows.alloc(std::max<size_t>(hr.size(), 1)));
+  PLATO_TRY(pl.hub_item0.alloc(std::max<size_t>(hr.size(), 1)));
+  PLATO_TRY(pl.hub_pieces.alloc(std::max<size_t>(hr.size(), 1)));
+  if (!items.empty())
+    PLATO_CUDA_TRY(cudaMemcpyAsync(pl.items.p, items.data(), items.size() * sizeof(uint2), cudaMemcpyHostToDevice, st));
+  if (!hr.empty()) {
+    PLATO_CUDA_TRY(cudaMemcpyAsync(pl.hub_rows.p, hr.data(), hr.size() * 4, cudaMemcpyHostToDevice, st));
+    PLATO_CUDA_TRY(cudaMemcpyAsync(pl.hub_item0.p, hi0.data(), hi0.size() * 4, cudaMemcpyHostToDevice, st));
+    PLATO_CUDA_TRY(cudaMemcpyAsync(pl.hub_pieces.p, hp.data(), hp.size() * 4, cudaMemcpyHostToDevice, st));
+  }
+  PLATO_CUDA_TRY(cudaStreamSynchronize(st));
+  const uint64_t n_short = static_cast<uint64_t>(V) - n_long - n_mid;
+  pl.blocks_long = static_cast<uint32_t>((static_cast<uint64_t>(pl.n_items) * 32 + 255) / 256);
+  pl.blocks_hubs = (pl.n_hubs + 255) / 256;
+  pl.blocks_mid = static_cast<uint32_t>((static_cast<uint64_t>(n_mid) * 8 + 255) / 256);
+  pl.blocks_short = static_cast<uint32_t>((n_short + 255) / 256);
+  pl.valid = true;
+  return PLATO_OK;
+}
+
 int ensure_ws(plato_graph* g, cudaStream_t st) {
   if (!g->rank_ws) {
     g->rank_ws = new (std::nothrow) rank_workspace();
@@ -74,6 +140,10 @@ int ensure_ws(plato_graph* g, cudaStream_t st) {
   }
   rank_workspace* ws = g->rank_ws;
   const uint32_t V = g->info.vertices;
+  if (!ws->plan_built) {
+    PLATO_TRY(build_plan(g, ws->plan, st));
+    ws->plan_built = true;
+  }
   PLATO_TRY(ensure_pull_tiles(g, cfg::kItems, st));
   if (ws->sms == 0) {
     int sms = 0;
@@ -85,13 +155,18 @@ int ensure_ws(plato_graph* g, cudaStream_t st) {
   PLATO_TRY(ws->x[1].alloc(V));
   PLATO_TRY(ws->carry.alloc(W));
   PLATO_TRY(ws->head.alloc(W));
-  // pull epochs: one partial per CTA + one per fixup block; dense epochs up to 148 * 8
-  PLATO_TRY(ws->partials.alloc(std::max<size_t>(ws->sms + (W + 255) / 256 + 1, 148 * 8)));
+  // pull epochs: one partial per CTA + one per fixup block (merge path) or one
+  // per block of each bin kernel; dense epochs up to 148 * 8
+  PLATO_TRY(ws->partials.alloc(std::max<size_t>(
+      {ws->sms + (W + 255) / 256 + 1, static_cast<size_t>(ws->plan.partials()) + 1, 148 * 8})));
   PLATO_TRY(ws->delta.alloc(1));
   if (!ws->h_delta) PLATO_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&ws->h_delta), sizeof(double)));
   uint32_t cap_a = 0, cap_b = 0;
   PLATO_TRY(set_pull_smem_attr<teleport_uniform>(g->device, &cap_a));
   PLATO_TRY(set_pull_smem_attr<teleport_single>(g->device, &cap_b));
+  uint32_t cap_c = 0;
+  PLATO_TRY(set_pull_smem_attr<teleport_seeds>(g->device, &cap_c));
+  cap_b = std::min(cap_b, cap_c);
   ws->hub_cap = std::min(cap_a, cap_b);
   return PLATO_OK;
 }
@@ -124,8 +199,39 @@ template <class Tele>
 int pull_epoch(plato_graph* g, const float* x, float* xn, Tele tele, float d, bool final_epoch,
                cudaStream_t st) {
   rank_workspace* ws = g->rank_ws;
-  const merge_tiles& mt = g->tiles.at(cfg::kItems);
   rank_update<Tele> upd{x, xn, g->out_deg.p, tele, d, final_epoch ? 1 : 0};
+  const pull_plan& pl = ws->plan;
+  if (pl.valid) {
+    const pull_plan_view pv{pl.n_long, pl.n_mid, g->info.vertices, pl.n_items, pl.items.p,
+                            pl.n_hubs, pl.hub_rows.p, pl.hub_item0.p, pl.hub_pieces.p,
+                            pl.piece_sum.p};
+    double* part = ws->partials.p;
+    if (pl.blocks_long) {
+      prof_scope ps("k_pull_long", st);
+      k_pull_long<rank_update<Tele>><<<pl.blocks_long, 256, 0, st>>>(pv, g->in_off.p, g->in_adj.p, x, upd, part);
+      PLATO_LAUNCHED("k_pull_long");
+    }
+    part += pl.blocks_long;
+    if (pl.blocks_hubs) {
+      prof_scope ps("k_pull_hubs", st);
+      k_pull_hubs<rank_update<Tele>><<<pl.blocks_hubs, 256, 0, st>>>(pv, upd, part);
+      PLATO_LAUNCHED("k_pull_hubs");
+    }
+    part += pl.blocks_hubs;
+    if (pl.blocks_mid) {
+      prof_scope ps("k_pull_mid", st);
+      k_pull_mid<rank_update<Tele>><<<pl.blocks_mid, 256, 0, st>>>(pv, g->in_off.p, g->in_adj.p, x, upd, part);
+      PLATO_LAUNCHED("k_pull_mid");
+    }
+    part += pl.blocks_mid;
+    if (pl.blocks_short) {
+      prof_scope ps("k_pull_short", st);
+      k_pull_short<rank_update<Tele>><<<pl.blocks_short, 256, 0, st>>>(pv, g->in_off.p, g->in_adj.p, x, upd, part);
+      PLATO_LAUNCHED("k_pull_short");
+    }
+    return PLATO_OK;
+  }
+  const merge_tiles& mt = g->tiles.at(cfg::kItems);
   const uint32_t H = std::min<uint32_t>(g->info.vertices, ws->hub_cap);
   pull_warp_args a{mt.row.p, mt.edge.p, mt.count, g->stored_edges, g->in_off.p, g->in_adj.p,
                    x, H, ws->carry.p, ws->head.p, ws->partials.p};
@@ -145,6 +251,7 @@ int pull_epoch(plato_graph* g, const float* x, float* xn, Tele tele, float d, bo
 }
 
 int partial_count(const plato_graph* g) {
+  if (g->rank_ws->plan.valid) return static_cast<int>(g->rank_ws->plan.partials());
   const uint32_t W = g->rank_ws->sms * cfg::kWarps;
   return static_cast<int>(g->rank_ws->sms + (W + 255) / 256);
 }
@@ -288,6 +395,80 @@ int ppr_impl(plato_graph* g, const plato_ppr_opts* o, int mode, float* d_out, cu
   return PLATO_OK;
 }
 
+// trustrank.hpp:197-206 with explicit seeds: x = (1/|S|)/deg on seeds (1/|S| if deg 0).
+__global__ void k_init_seeds(const uint32_t* __restrict__ deg, uint32_t V,
+                             const uint32_t* __restrict__ bits, float init, float* x) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    float val = 0.f;
+    if ((bits[v >> 5] >> (v & 31)) & 1u) {
+      const uint32_t dg = deg[v];
+      val = dg > 0 ? init / static_cast<float>(dg) : init;
+    }
+    x[v] = val;
+  }
+}
+
+__global__ void k_set_seed_bits(const uint32_t* __restrict__ seeds, uint32_t n, uint32_t* bits) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    atomicOr(bits + (seeds[i] >> 5), 1u << (seeds[i] & 31));
+}
+
+// Seed-set PPR, one query (algo::trustrank with the seeds given, pull-only).
+int seedset_impl(plato_graph* g, const uint32_t* seeds_ext, uint32_t n, const plato_ppr_opts* o,
+                 float* d_out, cudaStream_t st, plato_run_stats* stats) {
+  PLATO_TRY(check_rank_opts(o->iteration, o->damping));
+  const uint32_t V = g->info.vertices;
+  if (n == 0) return set_error(PLATO_EINVAL, "seedset ppr: empty seed set");
+  const std::vector<uint32_t>* to_int = nullptr;
+  PLATO_TRY(host_to_internal(g, &to_int, st));
+  std::vector<uint32_t> s;
+  s.reserve(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    if (seeds_ext[i] >= V) return set_error(PLATO_EINVAL, "seedset ppr: seed out of range");
+    s.push_back(to_int ? (*to_int)[seeds_ext[i]] : seeds_ext[i]);
+  }
+  std::sort(s.begin(), s.end());
+  s.erase(std::unique(s.begin(), s.end()), s.end());
+  PLATO_TRY(ensure_ws(g, st));
+  rank_workspace* ws = g->rank_ws;
+  PLATO_TRY(ws->seed_bits.alloc((V + 31) / 32));
+  PLATO_TRY(ws->seed_list.alloc(s.size()));
+  PLATO_CUDA_TRY(cudaMemsetAsync(ws->seed_bits.p, 0, ((V + 31) / 32) * sizeof(uint32_t), st));
+  PLATO_CUDA_TRY(cudaMemcpyAsync(ws->seed_list.p, s.data(), s.size() * sizeof(uint32_t),
+                                 cudaMemcpyHostToDevice, st));
+  k_set_seed_bits<<<grid_for(s.size(), 256), 256, 0, st>>>(ws->seed_list.p, static_cast<uint32_t>(s.size()),
+                                                           ws->seed_bits.p);
+  PLATO_LAUNCHED("k_set_seed_bits");
+  const float init = static_cast<float>(1.0 / static_cast<double>(s.size()));
+  k_init_seeds<<<grid_for(V, 256), 256, 0, st>>>(g->out_deg.p, V, ws->seed_bits.p, init, ws->x[0].p);
+  PLATO_LAUNCHED("k_init_seeds");
+  const float d = static_cast<float>(o->damping);
+  const teleport_seeds tele{ws->seed_bits.p,
+                            static_cast<float>((1.0 - o->damping) / static_cast<double>(s.size()))};
+  int cur = 0;
+  uint32_t epochs = 0;
+  double delta = 0.0;
+  for (uint32_t epoch = 0; epoch < o->iteration; ++epoch) {
+    const bool final_epoch = (epoch == o->iteration - 1);
+    PLATO_TRY(pull_epoch(g, ws->x[cur].p, ws->x[cur ^ 1].p, tele, d, final_epoch, st));
+    ++epochs;
+    if (!final_epoch && o->eps > 0.0) {
+      PLATO_TRY(read_delta(g, partial_count(g), st, &delta));
+      if (delta < o->eps) epoch = o->iteration - 2;
+    }
+    cur ^= 1;
+  }
+  PLATO_TRY(scatter_to_external_f32(g, ws->x[cur].p, d_out, st));
+  if (stats) {
+    *stats = plato_run_stats{};
+    stats->iterations = epochs;
+    stats->pull_iterations = epochs;
+    stats->delta = delta;
+  }
+  return PLATO_OK;
+}
+
 // Host-buffer wrapper: run into a device staging buffer, copy to `host`.
 template <class F>
 int with_host_output(plato_graph* g, float* host, F&& run) {
@@ -332,5 +513,15 @@ extern "C" int plato_personalized_pagerank(plato_graph* g, const plato_ppr_opts*
   PLATO_CUDA_TRY(cudaSetDevice(g->device));
   return with_host_output(g, ranks, [&](float* d_out, cudaStream_t st) {
     return ppr_impl(g, opts, mode, d_out, st, stats);
+  });
+}
+
+extern "C" int plato_seedset_ppr(plato_graph* g, const plato_vid_t* seeds, uint32_t n,
+                                 const plato_ppr_opts* opts, float* ranks, plato_run_stats* stats) {
+  if (!g || !seeds || !opts || !ranks) return set_error(PLATO_EINVAL, "plato_seedset_ppr: null argument");
+  std::lock_guard<std::mutex> lock(g->mu);
+  PLATO_CUDA_TRY(cudaSetDevice(g->device));
+  return with_host_output(g, ranks, [&](float* d_out, cudaStream_t st) {
+    return seedset_impl(g, seeds, n, opts, d_out, st, stats);
   });
 }
