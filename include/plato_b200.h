@@ -178,6 +178,27 @@ int plato_bfs(plato_graph* g, const plato_bfs_opts* opts, const plato_dualmode_o
 int plato_pagerank_device(plato_graph* g, const plato_pagerank_opts* opts, float* d_ranks,
                           void* stream, plato_run_stats* stats);
 
+/* ---- PageRank without allocation -----------------------------------------
+ * No counterpart in the reference.  For callers that must not have a library
+ * call cudaMalloc (an application whose pooling allocator owns all of HBM, a
+ * plugin under a fixed memory budget, a loop that cannot take an
+ * allocation's device-wide synchronisation): PageRank over the caller's own
+ * CSC in device memory (d_in_offsets [V+1], d_in_adj [edges] sources,
+ * d_out_degree [V]; edges = directed edges stored, both directions for an
+ * undirected graph), ranks written to device memory d_ranks [V] in the
+ * caller's vertex order, normalised as plato_pagerank, on `stream`.
+ * Every temporary lives in one static device array of
+ * PLATO_NOALLOC_SCRATCH_BYTES held by each GPU that loads the library until
+ * exit; a graph needing more (about 4V + 12(V+E)/224 bytes) gets EINVAL.
+ * The first call on a device looks up that array's device address (and sets
+ * the kernel's shared-memory limit); make it before any stream capture.
+ * Calls that overlap on the GPU race on the shared array: serialise them. */
+#define PLATO_NOALLOC_SCRATCH_BYTES (32u << 20)
+int plato_pagerank_csc_noalloc(uint32_t vertices, uint64_t edges, const uint64_t* d_in_offsets,
+                               const uint32_t* d_in_adj, const uint32_t* d_out_degree,
+                               const plato_pagerank_opts* opts, float* d_ranks, void* stream,
+                               plato_run_stats* stats);
+
 /* ---- batched multi-source personalized pagerank --------------------------
  * K queries, query q's seed set is seeds[seed_offsets[q] .. seed_offsets[q+1]).
  * Each query follows the seed-set semantics of algo::trustrank
