@@ -38,7 +38,9 @@ sys.path.insert(0, str(ROOT))
 SCALE, EDGEFACTOR, SEED = 24, 16, 3
 ITERATIONS, DAMPING = 20, 0.85
 METRIC = "PageRank GTEPS (RMAT s24 ef16, 20 iterations, pull)"
-PULL_KERNEL = "k_pull_warp"  # dominant kernel of a PageRank step
+# kernels of one pull epoch: the degree bins (relabelled graphs) or the merge path
+PULL_KERNELS = ["k_pull_long", "k_pull_mid", "k_pull_short", "k_pull_hubs", "k_pull_warp",
+                "k_pull_warp_fixup"]
 
 
 def env_rank():
@@ -93,6 +95,23 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
+def max_over_ranks(x: float, dist, device: str) -> float:
+    """Slowest rank's value (replicas are timed independently; the job is as
+    fast as its slowest replica).  `dist` is torch.distributed or None."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(units_per_rank: float, ms: float, world: int) -> float:
+    """Whole-job throughput of `world` replicas each processing
+    `units_per_rank` units in `ms` (the max over ranks)."""
+    return world * units_per_rank / (ms / 1e3)
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -104,6 +123,24 @@ def pr_algorithmic_bytes(V: int, E: int) -> int:
     """Bytes one pull epoch must move: column ids 4E + gathered ranks 4E +
     offsets 8(V+1) + x_old 4V + degree 4V + x_new 4V."""
     return 8 * E + 8 * (V + 1) + 12 * V
+
+
+def pull_bins(V: int, dst) -> dict:
+    """Per-kernel algorithmic bytes of one pull epoch on a graph relabelled by
+    descending in-degree (the bins of pull_binned.cuh: long > 32, mid 5..32,
+    short <= 4): each bin moves 8 bytes per edge (id + gathered rank) and
+    20 bytes per row (offset, x_old, degree, x_new)."""
+    indeg = np.sort(np.bincount(dst, minlength=V))[::-1].astype(np.int64)
+    n_long = int((indeg > 32).sum())
+    n_mid = int(((indeg > 4) & (indeg <= 32)).sum())
+    e_long = int(indeg[:n_long].sum())
+    e_mid = int(indeg[n_long:n_long + n_mid].sum())
+    e_short = int(indeg[n_long + n_mid:].sum())
+    n_short = V - n_long - n_mid
+    return {"k_pull_long": 8 * e_long + 20 * n_long, "k_pull_mid": 8 * e_mid + 20 * n_mid,
+            "k_pull_short": 8 * e_short + 20 * n_short, "k_pull_hubs": 0,
+            "rows": {"long": n_long, "mid": n_mid, "short": n_short},
+            "edges": {"long": e_long, "mid": e_mid, "short": e_short}}
 
 
 def cpu_pagerank_sample(V, src, dst, target_s=15.0):
@@ -215,17 +252,14 @@ def run_plato(args):
     launches = pb.kernel_launches() - launches0
     lib.plato_profile_enable(0)
     import ctypes as C
-    tot = C.c_double()
-    cnt = C.c_uint64()
-    lib.plato_profile_read(PULL_KERNEL.encode(), C.byref(tot), C.byref(cnt))
-    merge_ms, merge_n = tot.value, int(cnt.value)
-    lib.plato_profile_read((PULL_KERNEL + "_fixup").encode(), C.byref(tot), C.byref(cnt))
-    fix_ms = tot.value
-    ms = ev0.elapsed_time(ev1) / args.steps
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    kernel_times = {}
+    for name in PULL_KERNELS:
+        tot = C.c_double()
+        cnt = C.c_uint64()
+        lib.plato_profile_read(name.encode(), C.byref(tot), C.byref(cnt))
+        if cnt.value:
+            kernel_times[name] = (tot.value, int(cnt.value))
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dist, "cuda")
     value = world * E * ITERATIONS / (ms / 1e3) / 1e9
 
     # ---- end to end through the host-buffer C ABI ----------------------------
@@ -248,27 +282,45 @@ def run_plato(args):
         e2e_step()
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps, dist, "cuda")
     e2e_val = world * E * ITERATIONS / (e2e_ms / 1e3) / 1e9
 
     # ---- roofline of the dominant kernel -------------------------------------
     peak, peak_kind = measured_peak()
-    bytes_per_launch = pr_algorithmic_bytes(V, E)
-    per_launch_ms = merge_ms / max(merge_n, 1)
-    achieved = bytes_per_launch / (per_launch_ms / 1e3) / 1e9
+    epoch_bytes = pr_algorithmic_bytes(V, E)
+    bins = pull_bins(V, dst)
+    epochs = ITERATIONS * args.steps
+    per = {}
+    for name, (tot_ms, n) in kernel_times.items():
+        per[name] = {"launches": n, "ms_per_launch": tot_ms / n}
+        b = bins.get(name)
+        if b:
+            per[name]["bytes_per_launch"] = b
+            per[name]["achieved_gbs"] = b / (tot_ms / n / 1e3) / 1e9
+    epoch_ms = sum(t for t, _ in kernel_times.values()) / max(epochs, 1)
+    tot_k = sum(t for t, _ in kernel_times.values()) or 1.0
+    for name, (tot_ms, _) in kernel_times.items():
+        per[name]["share"] = tot_ms / tot_k
+    dom = max(kernel_times, key=lambda k: kernel_times[k][0]) if kernel_times else PULL_KERNELS[0]
+    if dom in bins and dom in per:
+        dom_bytes = bins[dom]
+        dom_ms = per[dom]["ms_per_launch"]
+    else:  # merge-path kernel: it is the whole epoch
+        dom_bytes = epoch_bytes
+        dom_ms = per.get(dom, {"ms_per_launch": epoch_ms})["ms_per_launch"]
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None, "kernel": PULL_KERNEL,
-            "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
-            "bytes_per_launch": bytes_per_launch, "launch_ms": per_launch_ms,
-            "fixup_ms_per_launch": fix_ms / max(merge_n, 1)}
-    prof = ROOT / "profiles" / "k_pull_warp_rmat_s24_traffic.json"
+            "frac": achieved / peak, "traffic": None, "kernel": dom,
+            "peak_source": f"{peak_kind} hbm_gbs (burst copy, of measured)",
+            "bytes_per_launch": dom_bytes, "launch_ms": dom_ms,
+            "pull_epoch": {"bytes": epoch_bytes, "ms": epoch_ms,
+                           "achieved": epoch_bytes / (epoch_ms / 1e3) / 1e9 if epoch_ms else None,
+                           "frac": (epoch_bytes / (epoch_ms / 1e3) / 1e9 / peak) if epoch_ms else None},
+            "kernels": per, "bins": {"rows": bins["rows"], "edges": bins["edges"]}}
+    prof = ROOT / "profiles" / f"{dom}_rmat_s{SCALE}_traffic.json"
     if prof.exists():
         tr = json.loads(prof.read_text())
-        roof["traffic"] = tr.get("dram_bytes_per_launch_full")
+        roof["traffic"] = tr.get("dram_bytes_per_launch")
 
     line = {
         "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
@@ -299,6 +351,171 @@ def run_plato(args):
     return 0
 
 
+def zipf_seed_sets(deg, K, max_size, seed):
+    """Seed-set sizes Zipf(s=1.5) clipped to [1, max_size], members uniform among deg > 0."""
+    rng = np.random.default_rng(seed)
+    cands = np.flatnonzero(deg > 0)
+    sizes = np.minimum(rng.zipf(1.5, K), max_size)
+    return [rng.choice(cands, int(n), replace=False).astype(np.uint32) for n in sizes]
+
+
+def suite_bfs(pb, roots_n=64):
+    """BFS on RMAT s22 ef16 symmetrised, seed 2: Graph500-style GTEPS (undirected
+    edges in the traversed component / time), harmonic mean over the roots."""
+    V, s, d = pb.rmat(22, 16, 2, symmetrize=True)
+    g = pb.Graph(V, s, d, is_directed=False)
+    deg = np.bincount(s, minlength=V) + np.bincount(d, minlength=V)
+    rng = np.random.default_rng(2)
+    roots = rng.choice(np.flatnonzero(deg > 0), roots_n, replace=False)
+    g.bfs(int(roots[0]), parents=False, levels=False)
+    teps, times, modes = [], [], []
+    for r in roots:
+        lev, _, st = g.bfs(int(r), parents=False)
+        m = int(deg[lev != pb.PLATO_LEVEL_UNREACHED].sum()) // 2
+        t0 = time.perf_counter()
+        _, _, st = g.bfs(int(r), parents=False, levels=False)
+        dt = time.perf_counter() - t0
+        teps.append(m / dt)
+        times.append(dt)
+        modes.append("".join("P" if x == "push" else "l" for x in st.mode_trace))
+    g.close()
+    hm = len(teps) / sum(1.0 / t for t in teps)
+    return {"workload": "bfs_rmat_s22_ef16_seed2_sym", "vertices": V, "undirected_edges": int(s.size),
+            "roots": roots_n, "gteps_harmonic_mean": hm / 1e9,
+            "ms_median": float(np.median(times)) * 1e3, "mode_trace_example": modes[0],
+            "timing": "host clock around plato_bfs (levels not copied back)"}
+
+
+def suite_ppr_single(pb):
+    """Single-source PPR on RMAT s24 seed 3 until L1 delta < 1e-7, both engines."""
+    V, s, d = pb.rmat(24, 16, 3)
+    g = pb.Graph(V, s, d, is_directed=True)
+    deg = np.bincount(s, minlength=V)
+    src = int(np.random.default_rng(3).choice(np.flatnonzero(deg > 0)))
+    out = {"workload": "ppr_rmat_s24_ef16_seed3", "src": src}
+    for mode, name in ((pb.PLATO_PPR_PULL, "pull"), (pb.PLATO_PPR_PUSHPULL, "pushpull")):
+        g.personalized_pagerank(src, 500, 0.85, 1e-7, mode)
+        t0 = time.perf_counter()
+        _, st = g.personalized_pagerank(src, 500, 0.85, 1e-7, mode)
+        dt = time.perf_counter() - t0
+        out[name] = {"ms": dt * 1e3, "iterations": st.iterations, "push_iterations": st.push_iterations}
+    g.close()
+    return out
+
+
+def suite_batch(pb, plain_n=16, quick=False):
+    """Batched multi-source PPR on RMAT s22 seed 4 (K in 64/256/1024, Zipf seed
+    sets 1..32, eps 1e-6) against the plain engine running the same queries one
+    at a time (plato_seedset_ppr, pull-only).  quick: one K=256 batch only (for
+    profiler captures)."""
+    V, s, d = pb.rmat(22, 16, 4)
+    g = pb.Graph(V, s, d, is_directed=True)
+    deg = np.bincount(s, minlength=V)
+    sets = zipf_seed_sets(deg, 1024, 32, 4)
+    if quick:
+        out = g.ppr_batch(sets[:256], 300, 0.85, 1e-6, topk=100)
+        g.close()
+        return {"workload": "ppr_batch_rmat_s22_ef16_seed4", "K": 256,
+                "iterations_max": int(out["iterations"].max())}
+    g.seedset_ppr(sets[0], 300, 0.85, 1e-6)
+    t0 = time.perf_counter()
+    plain_ranks = []
+    for q in range(plain_n):
+        r, _ = g.seedset_ppr(sets[q], 300, 0.85, 1e-6)
+        plain_ranks.append(r)
+    plain_qps = plain_n / (time.perf_counter() - t0)
+    res = {"workload": "ppr_batch_rmat_s22_ef16_seed4", "vertices": V, "edges": int(s.size),
+           "plain_qps": plain_qps, "plain_sample": plain_n}
+    for K in (64, 256, 1024):
+        g.ppr_batch(sets[:K], 300, 0.85, 1e-6, topk=100)  # autotune + warm
+        t0 = time.perf_counter()
+        out = g.ppr_batch(sets[:K], 300, 0.85, 1e-6, topk=100)
+        dt = time.perf_counter() - t0
+        res[f"K{K}"] = {"qps": K / dt, "s": dt, "speedup_vs_plain": K / dt / plain_qps,
+                        "iterations_max": int(out["iterations"].max())}
+        per_kt = {}
+        for kt in (8, 16, 32, 64):
+            if kt > max(8, K):
+                continue
+            g.ppr_batch(sets[:K], 300, 0.85, 1e-6, topk=100, k_tile=kt)
+            t0 = time.perf_counter()
+            g.ppr_batch(sets[:K], 300, 0.85, 1e-6, topk=100, k_tile=kt)
+            per_kt[kt] = K / (time.perf_counter() - t0)
+        res[f"K{K}"]["qps_by_k_tile"] = per_kt
+    chk = g.ppr_batch(sets[:plain_n], 300, 0.85, 1e-6, ranks=True)
+    l1 = [float(np.abs(chk["ranks"][q].astype(np.float64) - plain_ranks[q]).sum())
+          for q in range(plain_n)]
+    res["l1_batch_vs_plain_max"] = max(l1)
+    g.close()
+    return res
+
+
+def suite_serving(pb, rates=(100, 1000, 5000, 20000), n_req=400, slot_options=(64, 256)):
+    """PPR serving on RMAT s24 seed 5: Poisson arrivals, Zipf seed sets 1..64,
+    eps 1e-6, top-100; latency = completion - arrival (host clock)."""
+    V, s, d = pb.rmat(24, 16, 5)
+    g = pb.Graph(V, s, d, is_directed=True)
+    deg = np.bincount(s, minlength=V)
+    out = {"workload": "ppr_serving_rmat_s24_ef16_seed5", "vertices": V}
+    sets = zipf_seed_sets(deg, n_req, 64, 5)
+    # plain engine, one query at a time
+    g.seedset_ppr(sets[0], 300, 0.85, 1e-6)
+    t0 = time.perf_counter()
+    for q in range(8):
+        g.seedset_ppr(sets[q], 300, 0.85, 1e-6)
+    out["plain_qps"] = 8 / (time.perf_counter() - t0)
+    for slots in slot_options:
+        out[f"slots{slots}"] = _serve(pb, g, sets, rates, n_req, slots)
+    g.close()
+    return out
+
+
+def _serve(pb, g, sets, rates, n_req, slots):
+    out = {}
+    with pb.PPRServer(g, max_slots=slots, hbm_budget_bytes=64 << 30, max_iterations=300,
+                      eps=1e-6, topk=100) as srv:
+        for rate in rates:
+            rng = np.random.default_rng(rate)
+            arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+            sub, done, lat = 0, 0, []
+            ids = {}
+            t0 = time.perf_counter()
+            while done < n_req:
+                now = time.perf_counter() - t0
+                while sub < n_req and arrivals[sub] <= now:
+                    ids[srv.submit(sets[sub])] = arrivals[sub]
+                    sub += 1
+                st = srv.stats()
+                if st["live"] == 0 and st["queued"] == 0 and sub < n_req:
+                    time.sleep(max(0.0, arrivals[sub] - (time.perf_counter() - t0)))
+                    continue
+                srv.step()
+                while (r := srv.poll()) is not None:
+                    lat.append(time.perf_counter() - t0 - ids.pop(r[0]))
+                    done += 1
+            wall = time.perf_counter() - t0
+            lat_ms = np.array(lat) * 1e3
+            out[f"rate{rate}"] = {"offered_qps": rate, "sustained_qps": n_req / wall,
+                                  "p50_ms": float(np.percentile(lat_ms, 50)),
+                                  "p99_ms": float(np.percentile(lat_ms, 99))}
+    return out
+
+
+def run_suite(args):
+    import torch  # noqa: F401  (CUDA context for the library)
+    import plato_b200 as pb
+    res = {"suite": True}
+    for name, fn in (("bfs", suite_bfs), ("ppr_single", suite_ppr_single), ("ppr_batch", suite_batch),
+                     ("serving", suite_serving)):
+        if args.only and name not in args.only.split(","):
+            continue
+        t0 = time.perf_counter()
+        res[name] = fn(pb, quick=True) if (args.quick and name == "ppr_batch") else fn(pb)
+        res[name]["wall_s"] = time.perf_counter() - t0
+        print(json.dumps({name: res[name]}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -308,8 +525,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scale", type=int, default=SCALE,
                     help="RMAT scale (smaller values are for profiling captures only)")
+    ap.add_argument("--suite", action="store_true",
+                    help="also measure BFS, single PPR, batched PPR and serving (one JSON line each)")
+    ap.add_argument("--only", default="", help="with --suite: comma list of bfs,ppr_single,ppr_batch,serving")
+    ap.add_argument("--quick", action="store_true", help="with --suite: one small batch (profiling)")
     args = ap.parse_args()
     globals()["SCALE"] = args.scale
+    if args.suite:
+        return run_suite(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_plato(args)

@@ -260,15 +260,17 @@ class Graph:
               "plato_ppr_batch")
         return {"iterations": its, "ranks": out_r, "topk_ids": ids, "topk_vals": vals}
 
-    def bfs(self, root: int, push_threshold: float = 0.05, parents: bool = True):
-        """-> (levels uint32 [V] with PLATO_LEVEL_UNREACHED, parents or None, stats)."""
+    def bfs(self, root: int, push_threshold: float = 0.05, parents: bool = True,
+            levels: bool = True):
+        """-> (levels uint32 [V] with PLATO_LEVEL_UNREACHED or None, parents or None, stats)."""
         V = self.vertices
-        lev = np.empty(V, dtype=np.uint32)
+        lev = np.empty(V, dtype=np.uint32) if levels else None
         par = np.empty(V, dtype=np.uint32) if parents else None
         o = _lib.BfsOpts(root)
         eo = _lib.DualmodeOpts(push_threshold)
         s = _lib.RunStats()
-        check(self._lib.plato_bfs(self.handle, C.byref(o), C.byref(eo), _ptr(lev),
+        check(self._lib.plato_bfs(self.handle, C.byref(o), C.byref(eo),
+                                  _ptr(lev) if levels else None,
                                   _ptr(par) if parents else None, C.byref(s)), "plato_bfs")
         return lev, par, RunStats.from_c(s)
 

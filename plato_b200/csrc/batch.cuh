@@ -27,7 +27,7 @@ namespace plato_b200 {
 
 enum : uint8_t { COL_FREE = 0, COL_LIVE = 1, COL_FINAL = 2, COL_DONE = 3 };
 
-constexpr int kBatchTile = 4096;  // merge items per CTA (same tiles as the scalar pull)
+constexpr int kBatchTile = 1024;  // merge items per CTA: short per-group chains, many CTAs in flight
 
 struct seed_index_view {
   const uint32_t* off;   // [V+1] by internal vertex
@@ -87,11 +87,27 @@ __device__ __forceinline__ void ldvec(const float* p, float (&a)[VEC]) {
   }
 }
 
+// Evict-first variant for the state streams (old row read once, new row
+// written once): they must not push the hot gathered rows out of L2.
+template <int VEC>
+__device__ __forceinline__ void ldvec_cs(const float* p, float (&a)[VEC]) {
+  if constexpr (VEC == 4) {
+    const float4 t = __ldcs(reinterpret_cast<const float4*>(p));
+    a[0] = t.x;
+    a[1] = t.y;
+    a[2] = t.z;
+    a[3] = t.w;
+  } else {
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) a[c] = __ldcs(p + c);
+  }
+}
+
 // Update of one vertex row for this lane's VEC columns.
 template <int GL, int VEC>
 __device__ __forceinline__ void batch_finalize(const batch_pass& p, uint32_t v,
                                                const float (&y)[VEC], const uint8_t (&st)[VEC],
-                                               int lane_g, double (&dl)[VEC]) {
+                                               int lane_g, float (&dl)[VEC]) {
   constexpr int KT = GL * VEC;
   float tele[VEC];
 #pragma unroll
@@ -106,7 +122,7 @@ __device__ __forceinline__ void batch_finalize(const batch_pass& p, uint32_t v,
   const uint32_t dg = p.deg[v];
   const size_t base = static_cast<size_t>(v) * KT + lane_g * VEC;
   float old[VEC];
-  ldvec<VEC>(p.X + base, old);
+  ldvec_cs<VEC>(p.X + base, old);
 #pragma unroll
   for (int c = 0; c < VEC; ++c) {
     const float r = fmaf(p.d, y[c], tele[c]);
@@ -120,10 +136,10 @@ __device__ __forceinline__ void batch_finalize(const batch_pass& p, uint32_t v,
         xv = r;
         dlt = fabsf(xv - old[c]);
       }
-      p.Xn[base + c] = xv;
-      dl[c] += static_cast<double>(dlt);
+      __stcs(p.Xn + base + c, xv);
+      dl[c] += dlt;
     } else if (st[c] == COL_FINAL) {
-      p.Xn[base + c] = r;
+      __stcs(p.Xn + base + c, r);
     }
   }
 }
@@ -144,7 +160,7 @@ __device__ __forceinline__ void merge_search(const uint32_t* s_rowend, int nrows
 }
 
 template <int GL, int VEC>
-__global__ void __launch_bounds__(256) k_batch_pull(batch_pass p0) {
+__global__ void __launch_bounds__(256, 5) k_batch_pull(batch_pass p0) {
   constexpr int KT = GL * VEC, NG = 256 / GL, TILE = kBatchTile, IPG = TILE / NG;
   const batch_pass p = batch_tile_view<KT>(p0);
   __shared__ uint32_t s_rowend[TILE];
@@ -170,7 +186,7 @@ __global__ void __launch_bounds__(256) k_batch_pull(batch_pass p0) {
   const bool spans = p.off[i0] < j0;
   for (int r = threadIdx.x; r < nrows; r += 256)
     s_rowend[r] = static_cast<uint32_t>(p.off[i0 + r + 1] - j0);
-  for (int e = threadIdx.x; e < nnz; e += 256) s_src[e] = __ldg(p.adj + j0 + e);
+  for (int e = threadIdx.x; e < nnz; e += 256) s_src[e] = __ldcs(p.adj + j0 + e);
   __syncthreads();
 
   const int total = nrows + nnz;
@@ -181,17 +197,26 @@ __global__ void __launch_bounds__(256) k_batch_pull(batch_pass p0) {
   const int head = ra;
   bool head_done = false;
   float acc[VEC], head_acc[VEC];
-  double dl[VEC];
+  float dl[VEC];  // this lane's rows only; the CTA sums them in double
 #pragma unroll
   for (int c = 0; c < VEC; ++c) {
     acc[c] = 0.f;
     head_acc[c] = 0.f;
-    dl[c] = 0.0;
+    dl[c] = 0.f;
   }
   const float* xl = p.X + lane_g * VEC;
   int jj = ja;
   for (int r = ra; r <= rb; ++r) {
     const int e_end = (r < rb) ? static_cast<int>(s_rowend[r]) : jb;
+    for (; jj + 8 <= e_end; jj += 8) {  // eight row gathers in flight per lane
+      float a[8][VEC];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) ldvec<VEC>(xl + static_cast<size_t>(s_src[jj + u]) * KT, a[u]);
+#pragma unroll
+      for (int c = 0; c < VEC; ++c)
+        acc[c] += ((a[0][c] + a[1][c]) + (a[2][c] + a[3][c])) +
+                  ((a[4][c] + a[5][c]) + (a[6][c] + a[7][c]));
+    }
     for (; jj + 4 <= e_end; jj += 4) {
       float a0[VEC], a1[VEC], a2[VEC], a3[VEC];
       ldvec<VEC>(xl + static_cast<size_t>(s_src[jj]) * KT, a0);
@@ -275,9 +300,9 @@ __global__ void __launch_bounds__(256) k_batch_fixup(batch_pass p0) {
     mine |= (st[c] == COL_LIVE || st[c] == COL_FINAL);
   }
   if (!__syncthreads_or(mine)) return;
-  double dl[VEC];
+  float dl[VEC];
 #pragma unroll
-  for (int c = 0; c < VEC; ++c) dl[c] = 0.0;
+  for (int c = 0; c < VEC; ++c) dl[c] = 0.f;
   const uint32_t t = blockIdx.x * NG + g;
   if (t >= 1 && t < p.T) {
     const uint32_t i0 = p.trow[t];

@@ -65,6 +65,7 @@ class batch_engine {
   dbuf<uint32_t> counters_;  // [0] live, [1] retired count
   dbuf<uint32_t> retired_;
   uint32_t* h_counters_ = nullptr;
+  uint32_t h_counters_cap_ = 0;
   std::vector<uint32_t> h_retired_;
   // live seeds by column (internal ids), for the seed index
   std::vector<std::vector<uint32_t>> col_seeds_;

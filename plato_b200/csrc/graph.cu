@@ -343,6 +343,7 @@ int host_to_internal(plato_graph* g, const std::vector<uint32_t>** map, cudaStre
 }  // namespace plato_b200
 
 plato_graph::~plato_graph() {
+  plato_b200::destroy_batch_engine(batch_cache);
   plato_b200::destroy_rank_workspace(rank_ws);
   plato_b200::destroy_bfs_workspace(bfs_ws);
   if (stream) cudaStreamDestroy(stream);

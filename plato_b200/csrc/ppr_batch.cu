@@ -14,7 +14,9 @@ namespace {
 constexpr int kKernelsPerIteration = 4;
 
 bool kt_supported(uint32_t kt) { return kt == 8 || kt == 16 || kt == 32 || kt == 64 || kt == 128; }
-int group_lanes(uint32_t kt) { return kt <= 32 ? static_cast<int>(kt) : 32; }
+// Every lane gathers a float4 (4 columns, 16 bytes) per edge; kt/4 lanes
+// share one edge's kt-float row, so a warp gathers 128/kt edges per load.
+int group_lanes(uint32_t kt) { return static_cast<int>(kt / 4); }
 
 template <int GL, int VEC>
 int launch_pass(const batch_pass& p, uint32_t T, uint32_t fix_blocks, uint32_t ntiles,
@@ -88,6 +90,8 @@ batch_engine::~batch_engine() {
   if (h_counters_) cudaFreeHost(h_counters_);
 }
 
+void destroy_batch_engine(batch_engine* e) { delete e; }
+
 int batch_engine::init(uint32_t K, uint32_t kt, uint32_t max_iterations, double damping,
                        double eps, cudaStream_t st) {
   if (K == 0) return set_error(PLATO_EINVAL, "batched ppr: no queries");
@@ -127,8 +131,12 @@ int batch_engine::init(uint32_t K, uint32_t kt, uint32_t max_iterations, double 
   PLATO_CUDA_TRY(cudaMemsetAsync(parity_.p, 0, Kp_, st_));
   PLATO_CUDA_TRY(cudaMemsetAsync(iters_.p, 0, Kp_ * sizeof(uint32_t), st_));
   PLATO_CUDA_TRY(cudaMemsetAsync(seed_off_.p, 0, (static_cast<size_t>(V) + 1) * sizeof(uint32_t), st_));
-  if (!h_counters_)
+  if (!h_counters_ || h_counters_cap_ < 2 + Kp_) {
+    if (h_counters_) cudaFreeHost(h_counters_);
+    h_counters_ = nullptr;
     PLATO_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&h_counters_), (2 + Kp_) * sizeof(uint32_t)));
+    h_counters_cap_ = 2 + Kp_;
+  }
   col_seeds_.assign(Kp_, {});
   cur_ = 0;
   return capture();
@@ -159,10 +167,10 @@ int batch_engine::launch_iteration(int parity) {
   PLATO_CUDA_TRY(cudaMemsetAsync(counters_.p, 0, 2 * sizeof(uint32_t), st_));
   const uint32_t fix_blocks = rows_ - T;
   switch (kt_) {
-    case 8: PLATO_TRY((launch_pass<8, 1>(p, T, fix_blocks, ntiles_, st_))); break;
-    case 16: PLATO_TRY((launch_pass<16, 1>(p, T, fix_blocks, ntiles_, st_))); break;
-    case 32: PLATO_TRY((launch_pass<32, 1>(p, T, fix_blocks, ntiles_, st_))); break;
-    case 64: PLATO_TRY((launch_pass<32, 2>(p, T, fix_blocks, ntiles_, st_))); break;
+    case 8: PLATO_TRY((launch_pass<2, 4>(p, T, fix_blocks, ntiles_, st_))); break;
+    case 16: PLATO_TRY((launch_pass<4, 4>(p, T, fix_blocks, ntiles_, st_))); break;
+    case 32: PLATO_TRY((launch_pass<8, 4>(p, T, fix_blocks, ntiles_, st_))); break;
+    case 64: PLATO_TRY((launch_pass<16, 4>(p, T, fix_blocks, ntiles_, st_))); break;
     default: PLATO_TRY((launch_pass<32, 4>(p, T, fix_blocks, ntiles_, st_))); break;
   }
   k_batch_delta<<<dim3(kt_, ntiles_), 256, 0, st_>>>(partials_.p, rows_, kt_, state_.p, delta_.p);
@@ -479,7 +487,13 @@ extern "C" int plato_ppr_batch(plato_graph* g, uint32_t K, const uint64_t* seed_
   cudaStream_t st = g->stream;
   uint32_t kt = opts->k_tile;
   if (kt == 0) PLATO_TRY(batch_autotune(g, K, st, &kt));
-  batch_engine eng(g);
+  // the engine (and its V x K buffers) stays on the graph between calls, so a
+  // stream of batches pays for allocation and graph capture once
+  if (!g->batch_cache) {
+    g->batch_cache = new (std::nothrow) batch_engine(g);
+    if (!g->batch_cache) return set_error(PLATO_ENOMEM, "plato_ppr_batch: host allocation failed");
+  }
+  batch_engine& eng = *g->batch_cache;
   PLATO_TRY(eng.init(K, kt, opts->max_iterations, opts->damping, opts->eps, st));
   PLATO_TRY(eng.admit(cols, sets));
   uint32_t live = K;

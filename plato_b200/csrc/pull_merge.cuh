@@ -48,15 +48,20 @@ struct rank_update {
   Teleport tele;
   float d;
   int final_epoch;
+  // When set, the epoch kind is read from the device: 0 normal, 1 final
+  // (store r), 2 done (the kernels return at once); see k_epoch_control.
+  const int* mode = nullptr;
+
+  __device__ __forceinline__ bool skip() const { return mode && *mode == 2; }
 
   __device__ __forceinline__ double apply(uint32_t v, float y) const {
     const float r = fmaf(d, y, tele(v));
-    if (final_epoch) {
+    if (mode ? (*mode == 1) : (final_epoch != 0)) {
       xn[v] = r;
       return 0.0;
     }
-    const uint32_t dg = deg[v];
-    const float xo = x[v];
+    const uint32_t dg = __ldcs(deg + v);
+    const float xo = __ldcs(x + v);
     float xv, dl;
     if (dg > 0) {
       const float fd = static_cast<float>(dg);

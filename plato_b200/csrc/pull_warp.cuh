@@ -66,6 +66,7 @@ __global__ void __launch_bounds__(1024, 1) k_pull_warp(pull_warp_args a, Update 
   float* s_y = s_val + ITEMS;
   uint16_t* s_rowend = reinterpret_cast<uint16_t*>(s_y + ITEMS);
   __shared__ double s_red[32];
+  if (upd.skip()) return;  // device epoch control: nothing left to run
 
   {
     const float4* src4 = reinterpret_cast<const float4*>(a.x);
@@ -204,6 +205,7 @@ __global__ void __launch_bounds__(1024, 1) k_pull_warp(pull_warp_args a, Update 
 template <class Update>
 __global__ void __launch_bounds__(256) k_pull_warp_fixup(pull_warp_args a, uint32_t W, Update upd) {
   __shared__ double s_red[32];
+  if (upd.skip()) return;
   double dl = 0.0;
   const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= 1 && w < W) {

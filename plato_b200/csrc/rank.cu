@@ -9,6 +9,7 @@
 // final epoch (pagerank.hpp:137-139), so one more non-dividing epoch runs.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <new>
 #include <vector>
 
@@ -43,10 +44,14 @@ struct rank_workspace {
   bool plan_built = false;
   pull_plan plan;
   dbuf<uint32_t> seed_bits, seed_list;  // seed-set PPR
+  dbuf<float> out_stage;                // caller-id ranks before the copy to the host
+  dbuf<int> ctrl;                       // device epoch control (k_epoch_control)
   double* h_delta = nullptr;  // pinned
+  int* h_ctrl = nullptr;      // pinned [2]
   push_frontier frontier;
   ~rank_workspace() {
     if (h_delta) cudaFreeHost(h_delta);
+    if (h_ctrl) cudaFreeHost(h_ctrl);
   }
 };
 
@@ -125,10 +130,17 @@ int build_plan(plato_graph* g, pull_plan& pl, cudaStream_t st) {
   }
   PLATO_CUDA_TRY(cudaStreamSynchronize(st));
   const uint64_t n_short = static_cast<uint64_t>(V) - n_long - n_mid;
-  pl.blocks_long = static_cast<uint32_t>((static_cast<uint64_t>(pl.n_items) * 32 + 255) / 256);
-  pl.blocks_hubs = (pl.n_hubs + 255) / 256;
-  pl.blocks_mid = static_cast<uint32_t>((static_cast<uint64_t>(n_mid) * 8 + 255) / 256);
-  pl.blocks_short = static_cast<uint32_t>((n_short + 255) / 256);
+  // fixed grids of up to 8 CTAs (64 warps) per SM; the kernels stride over their work
+  int sms = 0;
+  PLATO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
+  const uint64_t cap = static_cast<uint64_t>(sms) * 8;
+  auto blocks = [cap](uint64_t threads) {
+    return static_cast<uint32_t>(std::min<uint64_t>((threads + 255) / 256, cap));
+  };
+  pl.blocks_long = blocks(static_cast<uint64_t>(pl.n_items) * 32);
+  pl.blocks_hubs = blocks(pl.n_hubs);
+  pl.blocks_mid = blocks(static_cast<uint64_t>(n_mid) * 8);
+  pl.blocks_short = blocks(n_short);
   pl.valid = true;
   return PLATO_OK;
 }
@@ -160,7 +172,9 @@ int ensure_ws(plato_graph* g, cudaStream_t st) {
   PLATO_TRY(ws->partials.alloc(std::max<size_t>(
       {ws->sms + (W + 255) / 256 + 1, static_cast<size_t>(ws->plan.partials()) + 1, 148 * 8})));
   PLATO_TRY(ws->delta.alloc(1));
+  PLATO_TRY(ws->ctrl.alloc(2));
   if (!ws->h_delta) PLATO_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&ws->h_delta), sizeof(double)));
+  if (!ws->h_ctrl) PLATO_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&ws->h_ctrl), 2 * sizeof(int)));
   uint32_t cap_a = 0, cap_b = 0;
   PLATO_TRY(set_pull_smem_attr<teleport_uniform>(g->device, &cap_a));
   PLATO_TRY(set_pull_smem_attr<teleport_single>(g->device, &cap_b));
@@ -197,9 +211,9 @@ __global__ void k_init_single(const uint32_t* __restrict__ deg, uint32_t V, uint
 // deltas to ws->partials (one per CTA, then one per fixup block).
 template <class Tele>
 int pull_epoch(plato_graph* g, const float* x, float* xn, Tele tele, float d, bool final_epoch,
-               cudaStream_t st) {
+               cudaStream_t st, const int* mode = nullptr) {
   rank_workspace* ws = g->rank_ws;
-  rank_update<Tele> upd{x, xn, g->out_deg.p, tele, d, final_epoch ? 1 : 0};
+  rank_update<Tele> upd{x, xn, g->out_deg.p, tele, d, final_epoch ? 1 : 0, mode};
   const pull_plan& pl = ws->plan;
   if (pl.valid) {
     const pull_plan_view pv{pl.n_long, pl.n_mid, g->info.vertices, pl.n_items, pl.items.p,
@@ -273,6 +287,54 @@ int check_rank_opts(uint32_t iteration, double damping) {
   return PLATO_OK;
 }
 
+// Pull-only epochs [start, iteration) from state x[*cur].  With eps == 0 the
+// schedule is known and nothing is read back.  With eps > 0 each epoch is
+// followed by k_epoch_control, which sums the delta on the device and sets
+// the next epoch's kind (pagerank.hpp:137-139); the host enqueues epochs in
+// batches and polls the control word between batches, so there is no host
+// round trip per epoch.  `scale` converts the delta to the reference's units.
+template <class Tele>
+int run_pull_epochs(plato_graph* g, Tele tele, float d, uint32_t iteration, uint32_t start,
+                    double eps, double scale, cudaStream_t st, int* cur, uint32_t* ran,
+                    double* delta) {
+  rank_workspace* ws = g->rank_ws;
+  *ran = 0;
+  if (start >= iteration) return PLATO_OK;
+  if (eps <= 0.0) {
+    for (uint32_t epoch = start; epoch < iteration; ++epoch) {
+      PLATO_TRY(pull_epoch(g, ws->x[*cur].p, ws->x[*cur ^ 1].p, tele, d, epoch == iteration - 1, st));
+      *cur ^= 1;
+      ++*ran;
+    }
+    return PLATO_OK;
+  }
+  const int init[2] = {start == iteration - 1 ? 1 : 0, static_cast<int>(start)};
+  PLATO_CUDA_TRY(cudaMemcpyAsync(ws->ctrl.p, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  const int cur0 = *cur;
+  constexpr uint32_t kBatch = 8;
+  uint32_t launched = 0;
+  const uint32_t nparts = static_cast<uint32_t>(partial_count(g));
+  while (start + launched < iteration) {
+    const uint32_t n = std::min(kBatch, iteration - start - launched);
+    for (uint32_t k = 0; k < n; ++k) {
+      const int c = (cur0 + static_cast<int>(launched + k)) & 1;
+      PLATO_TRY(pull_epoch(g, ws->x[c].p, ws->x[c ^ 1].p, tele, d, false, st, ws->ctrl.p));
+      k_epoch_control<<<1, 1024, 0, st>>>(ws->partials.p, nparts, ws->ctrl.p, ws->delta.p, scale,
+                                          eps, iteration);
+      PLATO_LAUNCHED("k_epoch_control");
+    }
+    launched += n;
+    PLATO_CUDA_TRY(cudaMemcpyAsync(ws->h_ctrl, ws->ctrl.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    PLATO_CUDA_TRY(cudaMemcpyAsync(ws->h_delta, ws->delta.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    PLATO_CUDA_TRY(cudaStreamSynchronize(st));
+    if (ws->h_ctrl[0] == 2) break;
+  }
+  *ran = static_cast<uint32_t>(ws->h_ctrl[1]) - start;
+  *cur = (cur0 + static_cast<int>(*ran)) & 1;
+  *delta = *ws->h_delta;
+  return PLATO_OK;
+}
+
 // PageRank into d_out (caller ids).  Internal buffers stay on the graph.
 int pagerank_impl(plato_graph* g, const plato_pagerank_opts* o, float* d_out, cudaStream_t st,
                   plato_run_stats* stats) {
@@ -287,17 +349,9 @@ int pagerank_impl(plato_graph* g, const plato_pagerank_opts* o, float* d_out, cu
   int cur = 0;
   uint32_t epochs = 0;
   double delta = 0.0;
-  for (uint32_t epoch = 0; epoch < o->iteration; ++epoch) {
-    const bool final_epoch = (epoch == o->iteration - 1);
-    PLATO_TRY(pull_epoch(g, ws->x[cur].p, ws->x[cur ^ 1].p, tele, d, final_epoch, st));
-    ++epochs;
-    if (!final_epoch && o->eps > 0.0) {
-      PLATO_TRY(read_delta(g, partial_count(g), st, &delta));
-      delta *= static_cast<double>(V);  // reference units (ranks summing to ~V)
-      if (delta < o->eps) epoch = o->iteration - 2;
-    }
-    cur ^= 1;
-  }
+  // reference units: the reference's ranks sum to ~V
+  PLATO_TRY(run_pull_epochs(g, tele, d, o->iteration, 0, o->eps, static_cast<double>(V), st, &cur,
+                            &epochs, &delta));
   PLATO_TRY(scatter_to_external_f32(g, ws->x[cur].p, d_out, st));
   if (stats) {
     *stats = plato_run_stats{};
@@ -352,37 +406,36 @@ int ppr_impl(plato_graph* g, const plato_ppr_opts* o, int mode, float* d_out, cu
   uint32_t epochs = 0, push_epochs = 0;
   uint64_t trace = 0;
   double delta = 0.0;
-  for (uint32_t epoch = 0; epoch < o->iteration; ++epoch) {
-    const bool final_epoch = (epoch == o->iteration - 1);
-    uint32_t nparts;
+  uint32_t epoch = 0;
+  // push phase (host-driven: the frontier decides), personalized_pagerank.hpp:184-239
+  for (; epoch < o->iteration; ++epoch) {
     if (!do_pull) {
       // personalized_pagerank.hpp:184-205: sticky switch on active_edges > edges/20
       uint64_t active_edges = 0;
       PLATO_TRY(frontier_active_edges(ws->frontier, st, &active_edges));
       do_pull = active_edges > edges / 20;
     }
-    if (do_pull) {
-      PLATO_TRY(pull_epoch(g, ws->x[cur].p, ws->x[cur ^ 1].p, tele, d, final_epoch, st));
-      nparts = partial_count(g);
-    } else {
-      PLATO_CUDA_TRY(cudaMemsetAsync(ws->y.p, 0, V * sizeof(float), st));
-      PLATO_TRY(frontier_push_scatter(ws->frontier, g, ws->x[cur].p, ws->y.p, st));
-      rank_update<teleport_single> upd{ws->x[cur].p, ws->x[cur ^ 1].p, g->out_deg.p, tele, d,
-                                       final_epoch ? 1 : 0};
-      k_dense_update<teleport_single><<<dense_blocks, 256, 0, st>>>(ws->y.p, V, upd,
-                                                                    ws->partials.p);
-      PLATO_LAUNCHED("k_dense_update");
-      nparts = dense_blocks;
-      if (epoch < 64) trace |= (1ull << epoch);
-      ++push_epochs;
-    }
+    if (do_pull) break;
+    const bool final_epoch = (epoch == o->iteration - 1);
+    PLATO_CUDA_TRY(cudaMemsetAsync(ws->y.p, 0, V * sizeof(float), st));
+    PLATO_TRY(frontier_push_scatter(ws->frontier, g, ws->x[cur].p, ws->y.p, st));
+    rank_update<teleport_single> upd{ws->x[cur].p, ws->x[cur ^ 1].p, g->out_deg.p, tele, d,
+                                     final_epoch ? 1 : 0};
+    k_dense_update<teleport_single><<<dense_blocks, 256, 0, st>>>(ws->y.p, V, upd, ws->partials.p);
+    PLATO_LAUNCHED("k_dense_update");
+    if (epoch < 64) trace |= (1ull << epoch);
+    ++push_epochs;
     ++epochs;
+    cur ^= 1;
     if (!final_epoch && o->eps > 0.0) {
-      PLATO_TRY(read_delta(g, nparts, st, &delta));
+      PLATO_TRY(read_delta(g, dense_blocks, st, &delta));
       if (delta < o->eps) epoch = o->iteration - 2;
     }
-    cur ^= 1;
   }
+  // pull phase (sticky): device-controlled epochs
+  uint32_t pulled = 0;
+  PLATO_TRY(run_pull_epochs(g, tele, d, o->iteration, epoch, o->eps, 1.0, st, &cur, &pulled, &delta));
+  epochs += pulled;
   PLATO_TRY(scatter_to_external_f32(g, ws->x[cur].p, d_out, st));
   if (stats) {
     *stats = plato_run_stats{};
@@ -449,16 +502,7 @@ int seedset_impl(plato_graph* g, const uint32_t* seeds_ext, uint32_t n, const pl
   int cur = 0;
   uint32_t epochs = 0;
   double delta = 0.0;
-  for (uint32_t epoch = 0; epoch < o->iteration; ++epoch) {
-    const bool final_epoch = (epoch == o->iteration - 1);
-    PLATO_TRY(pull_epoch(g, ws->x[cur].p, ws->x[cur ^ 1].p, tele, d, final_epoch, st));
-    ++epochs;
-    if (!final_epoch && o->eps > 0.0) {
-      PLATO_TRY(read_delta(g, partial_count(g), st, &delta));
-      if (delta < o->eps) epoch = o->iteration - 2;
-    }
-    cur ^= 1;
-  }
+  PLATO_TRY(run_pull_epochs(g, tele, d, o->iteration, 0, o->eps, 1.0, st, &cur, &epochs, &delta));
   PLATO_TRY(scatter_to_external_f32(g, ws->x[cur].p, d_out, st));
   if (stats) {
     *stats = plato_run_stats{};
@@ -473,7 +517,8 @@ int seedset_impl(plato_graph* g, const uint32_t* seeds_ext, uint32_t n, const pl
 template <class F>
 int with_host_output(plato_graph* g, float* host, F&& run) {
   cudaStream_t st = g->stream;
-  dbuf<float> out;
+  PLATO_TRY(ensure_ws(g, st));
+  dbuf<float>& out = g->rank_ws->out_stage;  // kept on the graph: no allocation per call
   PLATO_TRY(out.alloc(g->info.vertices));
   PLATO_TRY(run(out.p, st));
   PLATO_CUDA_TRY(cudaMemcpyAsync(host, out.p, g->info.vertices * sizeof(float),

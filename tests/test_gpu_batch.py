@@ -47,6 +47,23 @@ def test_batch_matches_oracle_per_query(g14):
         assert _l1(out["ranks"][q], want) <= L1_TOL, q
 
 
+@pytest.mark.parametrize("relabel", [True, False])
+def test_seedset_ppr_plain_engine(g14, relabel):
+    """The plain one-query engine (trustrank with explicit seeds, pull-only)."""
+    V, s, d, ref, g = g14
+    sets = zipf_seed_sets(ref.out_degrees(), 4, 32, 9)
+    with pb.Graph(V, s, d, True, relabel=relabel) as gg:
+        for S in sets:
+            want, ep, _ = ref.seedset_ppr(S, 300, 0.85, 1e-6)
+            got, st = gg.seedset_ppr(S, 300, 0.85, 1e-6)
+            assert abs(st.iterations - ep) <= 1
+            assert _l1(got, want) <= L1_TOL
+            fixed, st2 = gg.seedset_ppr(S, 17, 0.85, 0.0)
+            want2, ep2, _ = ref.seedset_ppr(S, 17, 0.85, 0.0)
+            assert st2.iterations == ep2 == 17
+            assert _l1(fixed, want2) <= L1_TOL
+
+
 def test_batch_fixed_iterations_exact_count(g14):
     V, s, d, ref, g = g14
     sets = zipf_seed_sets(ref.out_degrees(), 9, 8, 2)
