@@ -17,15 +17,47 @@
 
 namespace plato_b200 {
 
+// Device-side level state.  mode: 1 = the next level runs push, 0 = pull.
+struct bfs_control {
+  int mode;
+  int done;                  // the last level activated no vertex
+  uint32_t level;            // levels run (epochs, bfs.hpp:92)
+  uint32_t pushes;           // of which push
+  unsigned long long visited;
+  unsigned long long trace;  // bit i: level i ran push (first 64 levels)
+};
+
 struct bfs_workspace {
   push_frontier fr[2];
   dbuf<uint32_t> visited;
   dbuf<uint32_t> level, parent;
+  dbuf<bfs_control> ctrl;
+  bfs_control* h_ctrl = nullptr;  // pinned
+  ~bfs_workspace() {
+    if (h_ctrl) cudaFreeHost(h_ctrl);
+  }
 };
 
 void destroy_bfs_workspace(bfs_workspace* ws) { delete ws; }
 
 namespace {
+
+// After a level: count it, fold the new frontier into the visited count and
+// pick the next level's mode from its active-edge count (dualmode.hpp:264-279).
+__global__ void k_bfs_control(frontier_view fn, bfs_control* c, double edges, double threshold) {
+  if (threadIdx.x != 0 || c->done) return;
+  const unsigned long long actives = fn.counters[0];
+  if (c->mode == 1) c->pushes += 1;
+  c->level += 1;
+  c->visited += actives;
+  if (actives == 0) {
+    c->done = 1;
+    return;
+  }
+  const int push = (static_cast<double>(fn.counters[2]) / edges) < threshold ? 1 : 0;
+  c->mode = push;
+  if (push && c->level < 64) c->trace |= 1ull << c->level;
+}
 
 __global__ void k_bfs_init(uint32_t V, uint32_t root, uint32_t invalid_parent, uint32_t* level,
                            uint32_t* parent, uint32_t* visited) {
@@ -42,13 +74,15 @@ __global__ void k_bfs_init(uint32_t V, uint32_t root, uint32_t invalid_parent, u
 }
 
 // Push level: frontier chunks -> claim unvisited out-neighbours.
-__global__ void __launch_bounds__(256) k_bfs_push(frontier_view cur, unsigned long long nchunks,
-                                                  frontier_view next,
+__global__ void __launch_bounds__(256) k_bfs_push(frontier_view cur, frontier_view next,
                                                   const uint64_t* __restrict__ out_off,
                                                   const uint32_t* __restrict__ out_adj,
                                                   const uint32_t* __restrict__ deg,
                                                   uint32_t* visited, uint32_t* level,
-                                                  uint32_t* parent, uint32_t new_level) {
+                                                  uint32_t* parent, uint32_t new_level,
+                                                  const bfs_control* ctrl) {
+  if (ctrl->done || ctrl->mode != 1) return;  // uniform: pull level or finished
+  const unsigned long long nchunks = cur.counters[1];
   const unsigned lane = threadIdx.x & 31;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -82,7 +116,9 @@ __global__ void __launch_bounds__(256) k_bfs_pull(uint32_t V, frontier_view cur,
                                                   const uint32_t* __restrict__ in_adj,
                                                   const uint32_t* __restrict__ deg,
                                                   uint32_t* visited, uint32_t* level,
-                                                  uint32_t* parent, uint32_t new_level) {
+                                                  uint32_t* parent, uint32_t new_level,
+                                                  const bfs_control* ctrl) {
+  if (ctrl->done || ctrl->mode != 0) return;  // uniform: push level or finished
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t nrounds = (V + stride - 1) / stride;
   for (uint64_t r = 0; r < nrounds; ++r) {  // warp-uniform trip count for the appends
@@ -119,6 +155,9 @@ int ensure_bfs_ws(plato_graph* g) {
   PLATO_TRY(ws->visited.alloc((V + 31) / 32));
   PLATO_TRY(ws->level.alloc(V));
   PLATO_TRY(ws->parent.alloc(V));
+  PLATO_TRY(ws->ctrl.alloc(1));
+  if (!ws->h_ctrl)
+    PLATO_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&ws->h_ctrl), sizeof(bfs_control)));
   return PLATO_OK;
 }
 
@@ -150,46 +189,50 @@ int bfs_impl(plato_graph* g, const plato_bfs_opts* o, const plato_dualmode_opts*
   PLATO_TRY(frontier_seed(ws->fr[0], g, root, st));
   PLATO_TRY(frontier_read(ws->fr[0], st));
 
+  // Level loop with the engine switch on the device: after each level
+  // k_bfs_control reads the new frontier's counters, decides push or pull for
+  // the next level (dualmode.hpp:264-279) and flags the end (bfs.hpp:92, no
+  // vertex activated).  The host enqueues levels in batches and polls between
+  // batches; levels enqueued after the end return at once.
   const double edges = static_cast<double>(g->stored_edges);
-  int cur = 0;
-  uint64_t actives = 1, visited = 1, trace = 0;
-  uint32_t epoch = 0, push_epochs = 0;
+  const bool first_push = (static_cast<double>(ws->fr[0].h_counters[2]) / edges) < threshold;
+  const bfs_control init{first_push ? 1 : 0, 0, 0, 0, 1ull, first_push ? 1ull : 0ull};
+  PLATO_CUDA_TRY(cudaMemcpyAsync(ws->ctrl.p, &init, sizeof(init), cudaMemcpyHostToDevice, st));
+  const unsigned push_blocks = 148 * 16;
   const unsigned pull_blocks = grid_for(V, 256, 148 * 8);
-  while (actives != 0) {
-    push_frontier& fc = ws->fr[cur];
-    push_frontier& fn = ws->fr[cur ^ 1];
-    PLATO_TRY(frontier_reset(fn, V, st));
-    const uint64_t active_edges = fc.h_counters[2];
-    const bool is_sparse = (static_cast<double>(active_edges) / edges) < threshold;
-    if (is_sparse) {
-      const unsigned long long nchunks = fc.h_counters[1];
-      if (nchunks) {
-        k_bfs_push<<<grid_for(nchunks * 32, 256, 148 * 16), 256, 0, st>>>(
-            fc.view(), nchunks, fn.view(), g->out_off.p, g->out_adj.p, g->out_deg.p,
-            ws->visited.p, ws->level.p, ws->parent.p, epoch + 1);
-        PLATO_LAUNCHED("k_bfs_push");
-      }
-      if (epoch < 64) trace |= 1ull << epoch;
-      ++push_epochs;
-    } else {
+  constexpr uint32_t kBatch = 4;
+  uint32_t launched = 0;
+  for (;;) {
+    for (uint32_t k = 0; k < kBatch; ++k, ++launched) {
+      const int cur = static_cast<int>(launched & 1u);
+      push_frontier& fc = ws->fr[cur];
+      push_frontier& fn = ws->fr[cur ^ 1];
+      PLATO_TRY(frontier_reset(fn, V, st));
+      k_bfs_push<<<push_blocks, 256, 0, st>>>(fc.view(), fn.view(), g->out_off.p, g->out_adj.p,
+                                              g->out_deg.p, ws->visited.p, ws->level.p,
+                                              ws->parent.p, launched + 1, ws->ctrl.p);
+      PLATO_LAUNCHED("k_bfs_push");
       k_bfs_pull<<<pull_blocks, 256, 0, st>>>(V, fc.view(), fn.view(), g->in_off.p, g->in_adj.p,
                                               g->out_deg.p, ws->visited.p, ws->level.p,
-                                              ws->parent.p, epoch + 1);
+                                              ws->parent.p, launched + 1, ws->ctrl.p);
       PLATO_LAUNCHED("k_bfs_pull");
+      k_bfs_control<<<1, 32, 0, st>>>(fn.view(), ws->ctrl.p, edges, threshold);
+      PLATO_LAUNCHED("k_bfs_control");
     }
-    PLATO_TRY(frontier_read(fn, st));
-    actives = fn.h_counters[0];
-    visited += actives;
-    ++epoch;
-    cur ^= 1;
+    PLATO_CUDA_TRY(cudaMemcpyAsync(ws->h_ctrl, ws->ctrl.p, sizeof(bfs_control), cudaMemcpyDeviceToHost, st));
+    PLATO_CUDA_TRY(cudaStreamSynchronize(st));
+    if (ws->h_ctrl->done) break;
   }
+  const bfs_control& c = *ws->h_ctrl;
   if (stats) {
     *stats = plato_run_stats{};
-    stats->iterations = epoch;
-    stats->push_iterations = push_epochs;
-    stats->pull_iterations = epoch - push_epochs;
-    stats->visited = visited;
-    stats->mode_trace = trace;
+    stats->iterations = c.level;
+    const uint32_t traced = std::min<uint32_t>(c.level, 64);
+    const uint64_t mask = traced >= 64 ? ~0ull : ((1ull << traced) - 1);
+    stats->push_iterations = c.pushes;
+    stats->pull_iterations = c.level - c.pushes;
+    stats->visited = c.visited;
+    stats->mode_trace = c.trace & mask;
   }
   return PLATO_OK;
 }
