@@ -126,9 +126,20 @@ __global__ void __launch_bounds__(256) k_bfs_pull(uint32_t V, frontier_view cur,
     bool fresh = false;
     if (v < V && !test_bit(visited, static_cast<uint32_t>(v))) {
       const uint64_t b = in_off[v], e = in_off[v + 1];
-      for (uint64_t i = b; i < e; ++i) {
-        const uint32_t s = in_adj[i];
-        if (test_bit(cur.bits, s)) {
+      // four in-neighbours per step (ids, then bitmap tests, all in flight);
+      // the first hit in CSC order is the parent, as in a one-by-one scan
+      for (uint64_t i = b; i < e; i += 4) {
+        const bool p1 = i + 1 < e, p2 = i + 2 < e, p3 = i + 3 < e;
+        const uint32_t s0 = in_adj[i];
+        const uint32_t s1 = p1 ? in_adj[i + 1] : 0u;
+        const uint32_t s2 = p2 ? in_adj[i + 2] : 0u;
+        const uint32_t s3 = p3 ? in_adj[i + 3] : 0u;
+        const bool h0 = test_bit(cur.bits, s0);
+        const bool h1 = p1 && test_bit(cur.bits, s1);
+        const bool h2 = p2 && test_bit(cur.bits, s2);
+        const bool h3 = p3 && test_bit(cur.bits, s3);
+        if (h0 || h1 || h2 || h3) {
+          const uint32_t s = h0 ? s0 : h1 ? s1 : h2 ? s2 : s3;
           fresh = true;
           level[v] = new_level;
           parent[v] = s;

@@ -4,11 +4,12 @@
 //
 // The engine numbers vertices by descending in-degree, so the CSC columns fall
 // into three contiguous bins, each with its own work granularity:
-//   long   in-degree > kMidMax: one warp per work item, an item being a whole
-//          row or a kLongPiece-edge piece of a hub row; lanes stride the edges
-//          with four id loads and four rank gathers in flight each; pieces of
-//          one hub row are summed in piece order by k_pull_hubs.
-//   mid    kShortMax < in-degree <= kMidMax: 8 lanes per row.
+//   long   in-degree > kMidMax: one warp per work unit, a unit being a
+//          kLongPiece-edge piece of a hub row or a group of up to 32
+//          consecutive rows; the id loads of the next round of 128 edges
+//          overlap the rank gathers of this one; pieces of one hub row are
+//          summed in piece order by k_pull_hubs.
+//   mid    kShortMax < in-degree <= kMidMax: 8 lanes per row, one round.
 //   short  in-degree <= kShortMax (empty rows included): one thread per row.
 // Kernels run a fixed grid (a few CTAs per SM) and stride over their work, so
 // each writes one delta partial per CTA.  Per-edge work is an id load, a
@@ -32,7 +33,7 @@ constexpr uint32_t kLongPiece = 4096;
 struct pull_plan_view {
   uint32_t n_long, n_mid, V;      // rows [0,n_long) long, [n_long, n_long+n_mid) mid, rest short
   uint32_t n_items;               // long work items
-  const uint2* items;             // (row, piece)
+  const uint2* items;             // long-bin units (see k_pull_long)
   uint32_t n_hubs;                // rows of the long bin with more than one piece
   const uint32_t* hub_rows;       // [n_hubs]
   const uint32_t* hub_item0;      // [n_hubs] first item of the row
@@ -40,6 +41,33 @@ struct pull_plan_view {
   float* piece_sum;               // [n_items]
 };
 
+// Long-bin work units (pull_plan_view::items), hub pieces first:
+//   (row, kPieceFlag | k)  edges [k*kLongPiece, (k+1)*kLongPiece) of a hub row
+//   (row0, n)              rows [row0, row0+n), n <= 32, at most kGroupEdges
+//                          edges in all unless n == 1
+constexpr uint32_t kPieceFlag = 0x80000000u;
+constexpr uint32_t kGroupRows = 32;
+constexpr uint32_t kGroupEdges = 4096;
+
+// Ids of one round: edges [i, i+128) of the current segment clipped to e,
+// lane l taking i+l, i+l+32, i+l+64, i+l+96.
+struct round_ids {
+  uint32_t a0, a1, a2, a3;
+  __device__ __forceinline__ void load(const uint32_t* __restrict__ ab, uint32_t j, uint32_t e) {
+    a0 = j < e ? __ldcs(ab + j) : 0u;
+    a1 = j + 32 < e ? __ldcs(ab + j + 32) : 0u;
+    a2 = j + 64 < e ? __ldcs(ab + j + 64) : 0u;
+    a3 = j + 96 < e ? __ldcs(ab + j + 96) : 0u;
+  }
+};
+
+// One warp per unit.  A unit's segments (one hub piece, or up to 32 whole
+// rows) are walked in rounds of 128 edges, software-pipelined one round
+// deep: the ids of the next round (possibly of the next row) are loaded
+// before the ranks of this round are gathered, so an id load and a gather
+// overlap instead of running back to back.  Lane j keeps the sum of segment
+// j and applies the update of row row0+j, so the offsets, degrees and old
+// ranks of a group are read with one coalesced access each.
 template <class Update>
 __global__ void __launch_bounds__(256, 8) k_pull_long(pull_plan_view pv, const uint64_t* __restrict__ off,
                                                    const uint32_t* __restrict__ adj,
@@ -50,31 +78,70 @@ __global__ void __launch_bounds__(256, 8) k_pull_long(pull_plan_view pv, const u
   const unsigned lane = threadIdx.x & 31;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   double dl = 0.0;
-  for (uint32_t item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; item < pv.n_items;
-       item += nwarps) {
-    const uint2 it = pv.items[item];
-    const uint64_t rb = __ldcs(off + it.x), re = __ldcs(off + it.x + 1);
-    const uint64_t b = rb + static_cast<uint64_t>(it.y) * kLongPiece;
-    const uint64_t e = min(b + kLongPiece, re);
-    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
-    uint64_t i = b + lane;
-    for (; i + 96 < e; i += 128) {
-      const uint32_t a0 = __ldcs(adj + i), a1 = __ldcs(adj + i + 32), a2 = __ldcs(adj + i + 64),
-                     a3 = __ldcs(adj + i + 96);
-      s0 += __ldg(x + a0);
-      s1 += __ldg(x + a1);
-      s2 += __ldg(x + a2);
-      s3 += __ldg(x + a3);
+  uint32_t unit = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint2 it = unit < pv.n_items ? pv.items[unit] : make_uint2(0, 0);
+  for (; unit < pv.n_items; unit += nwarps) {
+    const uint32_t un = unit + nwarps;
+    const uint2 it_next = un < pv.n_items ? pv.items[un] : make_uint2(0, 0);
+    const bool piece = (it.y & kPieceFlag) != 0;
+    const uint32_t nseg = piece ? 1u : it.y;
+    uint64_t base;
+    uint32_t sb = 0, se = 0;  // this lane's segment, relative to base
+    if (piece) {
+      const uint64_t rb = __ldcs(off + it.x), re = __ldcs(off + it.x + 1);
+      base = rb + static_cast<uint64_t>(it.y & ~kPieceFlag) * kLongPiece;
+      if (lane == 0) se = static_cast<uint32_t>(min(static_cast<uint64_t>(kLongPiece), re - base));
+    } else {
+      uint64_t lo = 0, hi = 0;
+      if (lane < nseg) {
+        lo = __ldcs(off + it.x + lane);
+        hi = __ldcs(off + it.x + lane + 1);
+      }
+      base = __shfl_sync(0xffffffffu, lo, 0);
+      sb = static_cast<uint32_t>(lo - base);
+      se = static_cast<uint32_t>(hi - base);
     }
-    for (; i < e; i += 32) s0 += __ldg(x + __ldcs(adj + i));
-    float s = (s0 + s1) + (s2 + s3);
-    s = warp_sum(s);
-    if (lane == 0) {
-      if (re - rb <= kLongPiece)
-        dl += upd.apply(it.x, s);
-      else
-        pv.piece_sum[item] = s;
+    const uint32_t* ab = adj + base;
+    uint32_t k = 0;
+    uint32_t i = __shfl_sync(0xffffffffu, sb, 0), e = __shfl_sync(0xffffffffu, se, 0);
+    round_ids cur;
+    cur.load(ab, i + lane, e);
+    float s = 0.f, res = 0.f;
+    for (;;) {
+      // cursor of the next round (warp-uniform)
+      uint32_t kn = k, in = i + 128, en = e;
+      if (in >= e) {
+        kn = k + 1;
+        const uint32_t src = kn < nseg ? kn : 0;
+        in = __shfl_sync(0xffffffffu, sb, src);
+        en = __shfl_sync(0xffffffffu, se, src);
+      }
+      const bool more = kn < nseg;
+      round_ids nxt{0u, 0u, 0u, 0u};
+      if (more) nxt.load(ab, in + lane, en);
+      const uint32_t j = i + lane;
+      const float g0 = j < e ? __ldg(x + cur.a0) : 0.f;
+      const float g1 = j + 32 < e ? __ldg(x + cur.a1) : 0.f;
+      const float g2 = j + 64 < e ? __ldg(x + cur.a2) : 0.f;
+      const float g3 = j + 96 < e ? __ldg(x + cur.a3) : 0.f;
+      s += (g0 + g1) + (g2 + g3);
+      if (kn != k) {
+        const float t = warp_sum(s);
+        if (lane == k) res = t;
+        s = 0.f;
+      }
+      if (!more) break;
+      cur = nxt;
+      k = kn;
+      i = in;
+      e = en;
     }
+    if (piece) {
+      if (lane == 0) pv.piece_sum[unit] = res;
+    } else if (lane < nseg) {
+      dl += upd.apply(it.x + lane, res);
+    }
+    it = it_next;
   }
   dl = block_sum<256>(dl, s_red);
   if (threadIdx.x == 0) partials[blockIdx.x] = dl;
@@ -115,9 +182,19 @@ __global__ void __launch_bounds__(256) k_pull_mid(pull_plan_view pv, const uint6
     float s = 0.f;
     uint32_t v = 0;
     if (valid) {
+      // a mid row has at most 32 edges: one predicated round of 4 per lane
+      static_assert(kMidMax <= 32, "k_pull_mid covers a row in one round of 8 lanes x 4");
       v = pv.n_long + r;
       const uint64_t b = __ldcs(off + v), e = __ldcs(off + v + 1);
-      for (uint64_t i = b + sub; i < e; i += 8) s += __ldg(x + __ldcs(adj + i));
+      const uint64_t i = b + sub;
+      const bool p0 = i < e, p1 = i + 8 < e, p2 = i + 16 < e, p3 = i + 24 < e;
+      const uint32_t a0 = p0 ? __ldcs(adj + i) : 0u;
+      const uint32_t a1 = p1 ? __ldcs(adj + i + 8) : 0u;
+      const uint32_t a2 = p2 ? __ldcs(adj + i + 16) : 0u;
+      const uint32_t a3 = p3 ? __ldcs(adj + i + 24) : 0u;
+      const float g0 = p0 ? __ldg(x + a0) : 0.f, g1 = p1 ? __ldg(x + a1) : 0.f;
+      const float g2 = p2 ? __ldg(x + a2) : 0.f, g3 = p3 ? __ldg(x + a3) : 0.f;
+      s = (g0 + g1) + (g2 + g3);
     }
     s += __shfl_xor_sync(0xffffffffu, s, 4);
     s += __shfl_xor_sync(0xffffffffu, s, 2);
@@ -140,9 +217,17 @@ __global__ void __launch_bounds__(256) k_pull_short(pull_plan_view pv, const uin
   for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; base + r < pv.V;
        r += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t v = static_cast<uint32_t>(base + r);
+    // at most kShortMax edges: all id loads, then all gathers, predicated
+    static_assert(kShortMax <= 4, "k_pull_short covers a row in one round of 4");
     const uint64_t b = __ldcs(off + v), e = __ldcs(off + v + 1);
-    float s = 0.f;
-    for (uint64_t i = b; i < e; ++i) s += __ldg(x + __ldcs(adj + i));
+    const bool p0 = b < e, p1 = b + 1 < e, p2 = b + 2 < e, p3 = b + 3 < e;
+    const uint32_t a0 = p0 ? __ldcs(adj + b) : 0u;
+    const uint32_t a1 = p1 ? __ldcs(adj + b + 1) : 0u;
+    const uint32_t a2 = p2 ? __ldcs(adj + b + 2) : 0u;
+    const uint32_t a3 = p3 ? __ldcs(adj + b + 3) : 0u;
+    const float g0 = p0 ? __ldg(x + a0) : 0.f, g1 = p1 ? __ldg(x + a1) : 0.f;
+    const float g2 = p2 ? __ldg(x + a2) : 0.f, g3 = p3 ? __ldg(x + a3) : 0.f;
+    const float s = (g0 + g1) + (g2 + g3);
     dl += upd.apply(v, s);
   }
   dl = block_sum<256>(dl, s_red);

@@ -101,16 +101,29 @@ int build_plan(plato_graph* g, pull_plan& pl, cudaStream_t st) {
   uint32_t n_long = 0, n_mid = 0;
   while (n_long < V && deg[n_long] > kMidMax) ++n_long;
   while (n_long + n_mid < V && deg[n_long + n_mid] > kShortMax) ++n_mid;
+  // long-bin units: the pieces of every hub row, then groups of consecutive
+  // rows (up to kGroupRows rows and kGroupEdges edges, at least one row)
   std::vector<uint2> items;
   std::vector<uint32_t> hr, hi0, hp;
   for (uint32_t r = 0; r < n_long; ++r) {
     const uint32_t pieces = (deg[r] + kLongPiece - 1) / kLongPiece;
-    if (pieces > 1) {
-      hr.push_back(r);
-      hi0.push_back(static_cast<uint32_t>(items.size()));
-      hp.push_back(pieces);
+    if (pieces <= 1) continue;
+    hr.push_back(r);
+    hi0.push_back(static_cast<uint32_t>(items.size()));
+    hp.push_back(pieces);
+    for (uint32_t k = 0; k < pieces; ++k) items.push_back(make_uint2(r, kPieceFlag | k));
+  }
+  for (uint32_t r = 0; r < n_long;) {
+    if (deg[r] > kLongPiece) {
+      ++r;
+      continue;
     }
-    for (uint32_t k = 0; k < pieces; ++k) items.push_back(make_uint2(r, k));
+    uint32_t n = 0, edges = 0;
+    while (r + n < n_long && n < kGroupRows && deg[r + n] <= kLongPiece &&
+           (n == 0 || edges + deg[r + n] <= kGroupEdges))
+      edges += deg[r + n++];
+    items.push_back(make_uint2(r, n));
+    r += n;
   }
   pl.n_long = n_long;
   pl.n_mid = n_mid;
