@@ -39,8 +39,8 @@ SCALE, EDGEFACTOR, SEED = 24, 16, 3
 ITERATIONS, DAMPING = 20, 0.85
 METRIC = "PageRank GTEPS (RMAT s24 ef16, 20 iterations, pull)"
 # kernels of one pull epoch: the degree bins (relabelled graphs) or the merge path
-PULL_KERNELS = ["k_pull_long", "k_pull_mid", "k_pull_short", "k_pull_hubs", "k_pull_warp",
-                "k_pull_warp_fixup"]
+PULL_KERNELS = ["k_pull_long", "k_pull_rows16", "k_pull_rows8", "k_pull_rows4", "k_pull_short",
+                "k_pull_hubs", "k_pull_warp", "k_pull_warp_fixup"]
 
 
 def env_rank():
@@ -127,20 +127,21 @@ def pr_algorithmic_bytes(V: int, E: int) -> int:
 
 def pull_bins(V: int, dst) -> dict:
     """Per-kernel algorithmic bytes of one pull epoch on a graph relabelled by
-    descending in-degree (the bins of pull_binned.cuh: long > 32, mid 5..32,
-    short <= 4): each bin moves 8 bytes per edge (id + gathered rank) and
-    20 bytes per row (offset, x_old, degree, x_new)."""
+    descending in-degree (the bins of pull_binned.cuh: long > 64, then
+    33..64, 17..32 and 5..16 for k_pull_rows16/8/4, short <= 4): each bin
+    moves 8 bytes per edge (id + gathered rank) and 20 bytes per row (offset,
+    x_old, degree, x_new)."""
     indeg = np.sort(np.bincount(dst, minlength=V))[::-1].astype(np.int64)
-    n_long = int((indeg > 32).sum())
-    n_mid = int(((indeg > 4) & (indeg <= 32)).sum())
-    e_long = int(indeg[:n_long].sum())
-    e_mid = int(indeg[n_long:n_long + n_mid].sum())
-    e_short = int(indeg[n_long + n_mid:].sum())
-    n_short = V - n_long - n_mid
-    return {"k_pull_long": 8 * e_long + 20 * n_long, "k_pull_mid": 8 * e_mid + 20 * n_mid,
-            "k_pull_short": 8 * e_short + 20 * n_short, "k_pull_hubs": 0,
-            "rows": {"long": n_long, "mid": n_mid, "short": n_short},
-            "edges": {"long": e_long, "mid": e_mid, "short": e_short}}
+    bounds = [("k_pull_long", 64, None), ("k_pull_rows16", 32, 64), ("k_pull_rows8", 16, 32),
+              ("k_pull_rows4", 4, 16), ("k_pull_short", -1, 4)]
+    out, rows, edges = {"k_pull_hubs": 0}, {}, {}
+    for name, lo, hi in bounds:
+        m = indeg > lo if hi is None else (indeg > lo) & (indeg <= hi)
+        n, e = int(m.sum()), int(indeg[m].sum())
+        out[name] = 8 * e + 20 * n
+        rows[name], edges[name] = n, e
+    out["rows"], out["edges"] = rows, edges
+    return out
 
 
 def cpu_pagerank_sample(V, src, dst, target_s=15.0):

@@ -3,13 +3,15 @@
 // with the update of pagerank.hpp:118-135).
 //
 // The engine numbers vertices by descending in-degree, so the CSC columns fall
-// into three contiguous bins, each with its own work granularity:
-//   long   in-degree > kMidMax: one warp per work unit, a unit being a
+// into contiguous bins, each with its own work granularity:
+//   long   in-degree > 64: one warp per work unit, a unit being a
 //          kLongPiece-edge piece of a hub row or a group of up to 32
 //          consecutive rows; the id loads of the next round of 128 edges
 //          overlap the rank gathers of this one; pieces of one hub row are
 //          summed in piece order by k_pull_hubs.
-//   mid    kShortMax < in-degree <= kMidMax: 8 lanes per row, one round.
+//   rows   33..64, 17..32, 5..16: k_pull_rows with 16, 8 or 4 lanes per
+//          row, each row in one round of four edges per lane, rounds
+//          pipelined the same way.
 //   short  in-degree <= kShortMax (empty rows included): one thread per row.
 // Kernels run a fixed grid (a few CTAs per SM) and stride over their work, so
 // each writes one delta partial per CTA.  Per-edge work is an id load, a
@@ -27,11 +29,11 @@
 namespace plato_b200 {
 
 constexpr uint32_t kShortMax = 4;
-constexpr uint32_t kMidMax = 32;
+constexpr uint32_t kRowsMax[3] = {64, 32, 16};  // k_pull_rows<16>, <8>, <4>: in-degree <= 4 * LPR
 constexpr uint32_t kLongPiece = 4096;
 
 struct pull_plan_view {
-  uint32_t n_long, n_mid, V;      // rows [0,n_long) long, [n_long, n_long+n_mid) mid, rest short
+  uint32_t n_long, short_begin, V;  // rows [0,n_long) long, [short_begin, V) short
   uint32_t n_items;               // long work items
   const uint2* items;             // long-bin units (see k_pull_long)
   uint32_t n_hubs;                // rows of the long bin with more than one piece
@@ -101,6 +103,8 @@ __global__ void __launch_bounds__(256, 8) k_pull_long(pull_plan_view pv, const u
       sb = static_cast<uint32_t>(lo - base);
       se = static_cast<uint32_t>(hi - base);
     }
+    const bool mine = !piece && lane < nseg;
+    const typename Update::operands ops = upd.load(mine ? it.x + lane : it.x);
     const uint32_t* ab = adj + base;
     uint32_t k = 0;
     uint32_t i = __shfl_sync(0xffffffffu, sb, 0), e = __shfl_sync(0xffffffffu, se, 0);
@@ -138,8 +142,8 @@ __global__ void __launch_bounds__(256, 8) k_pull_long(pull_plan_view pv, const u
     }
     if (piece) {
       if (lane == 0) pv.piece_sum[unit] = res;
-    } else if (lane < nseg) {
-      dl += upd.apply(it.x + lane, res);
+    } else if (mine) {
+      dl += upd.apply(it.x + lane, res, ops);
     }
     it = it_next;
   }
@@ -152,54 +156,105 @@ __global__ void __launch_bounds__(256) k_pull_hubs(pull_plan_view pv, Update upd
                                                    double* __restrict__ partials) {
   __shared__ double s_red[32];
   if (upd.skip()) return;
+  // one warp per hub row: lane l sums pieces l, l+32, ..., then a butterfly
+  // (a fixed order, so the row sum is reproducible)
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   double dl = 0.0;
-  for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < pv.n_hubs; h += gridDim.x * blockDim.x) {
+  for (uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < pv.n_hubs; h += nwarps) {
     const uint32_t i0 = pv.hub_item0[h], n = pv.hub_pieces[h];
     float y = 0.f;
-    for (uint32_t k = 0; k < n; ++k) y += pv.piece_sum[i0 + k];
-    dl += upd.apply(pv.hub_rows[h], y);
+    for (uint32_t k = lane; k < n; k += 32) y += pv.piece_sum[i0 + k];
+    y = warp_sum(y);
+    if (lane == 0) dl += upd.apply(pv.hub_rows[h], y);
   }
   dl = block_sum<256>(dl, s_red);
   if (threadIdx.x == 0) partials[blockIdx.x] = dl;
 }
 
-template <class Update>
-__global__ void __launch_bounds__(256) k_pull_mid(pull_plan_view pv, const uint64_t* __restrict__ off,
-                                                  const uint32_t* __restrict__ adj,
-                                                  const float* __restrict__ x, Update upd,
-                                                  double* __restrict__ partials) {
+// Ids of one single-round row: edges b+q, b+q+LPR, b+q+2*LPR, b+q+3*LPR
+// clipped to e (lane q of the row's LPR lanes).
+template <int LPR>
+struct row_ids {
+  uint32_t a0, a1, a2, a3;
+  __device__ __forceinline__ void load(const uint32_t* __restrict__ ab, uint32_t j, uint32_t e) {
+    a0 = j < e ? __ldcs(ab + j) : 0u;
+    a1 = j + LPR < e ? __ldcs(ab + j + LPR) : 0u;
+    a2 = j + 2 * LPR < e ? __ldcs(ab + j + 2 * LPR) : 0u;
+    a3 = j + 3 * LPR < e ? __ldcs(ab + j + 3 * LPR) : 0u;
+  }
+};
+
+// Rows [r0, r1) whose in-degree is at most 4*LPR.  One warp per unit of 32
+// consecutive rows; a round gives each row LPR lanes with four edges each, so
+// it covers 32/LPR rows and a unit takes LPR rounds.  The ids of the next
+// round are loaded while the ranks of this round are gathered; the offsets of
+// the warp's next unit and the update operands of this unit are loaded at the
+// start of the unit.  Lane j ends up with the sum of row row0+j, so offsets,
+// operands and new ranks move with one coalesced access each.
+template <int LPR, class Update>
+__global__ void __launch_bounds__(256, 8) k_pull_rows(uint32_t r0, uint32_t r1, const uint64_t* __restrict__ off,
+                                                   const uint32_t* __restrict__ adj,
+                                                   const float* __restrict__ x, Update upd,
+                                                   double* __restrict__ partials) {
+  static_assert(LPR == 4 || LPR == 8 || LPR == 16, "k_pull_rows: 4, 8 or 16 lanes per row");
+  constexpr uint32_t RPR = 32 / LPR;  // rows per round
   __shared__ double s_red[32];
   if (upd.skip()) return;
-  const unsigned sub = threadIdx.x & 7;
-  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
-  // warp-uniform trip count: the shuffles below need all 32 lanes
-  const uint32_t g0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-  const uint32_t rounds = (pv.n_mid + ngroups - 1) / ngroups;
+  const unsigned lane = threadIdx.x & 31, slot = lane / LPR, q = lane % LPR;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t n_units = (r1 - r0 + 31) / 32;
   double dl = 0.0;
-  for (uint32_t k = 0; k < rounds; ++k) {
-    const uint32_t r = g0 + k * ngroups;
-    const bool valid = r < pv.n_mid;
-    float s = 0.f;
-    uint32_t v = 0;
-    if (valid) {
-      // a mid row has at most 32 edges: one predicated round of 4 per lane
-      static_assert(kMidMax <= 32, "k_pull_mid covers a row in one round of 8 lanes x 4");
-      v = pv.n_long + r;
-      const uint64_t b = __ldcs(off + v), e = __ldcs(off + v + 1);
-      const uint64_t i = b + sub;
-      const bool p0 = i < e, p1 = i + 8 < e, p2 = i + 16 < e, p3 = i + 24 < e;
-      const uint32_t a0 = p0 ? __ldcs(adj + i) : 0u;
-      const uint32_t a1 = p1 ? __ldcs(adj + i + 8) : 0u;
-      const uint32_t a2 = p2 ? __ldcs(adj + i + 16) : 0u;
-      const uint32_t a3 = p3 ? __ldcs(adj + i + 24) : 0u;
-      const float g0 = p0 ? __ldg(x + a0) : 0.f, g1 = p1 ? __ldg(x + a1) : 0.f;
-      const float g2 = p2 ? __ldg(x + a2) : 0.f, g3 = p3 ? __ldg(x + a3) : 0.f;
-      s = (g0 + g1) + (g2 + g3);
+  uint32_t unit = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint64_t lo = 0, hi = 0;
+  if (unit < n_units && r0 + unit * 32 + lane < r1) {
+    lo = __ldcs(off + r0 + unit * 32 + lane);
+    hi = __ldcs(off + r0 + unit * 32 + lane + 1);
+  }
+  for (; unit < n_units; unit += nwarps) {
+    const uint32_t row0 = r0 + unit * 32, un = unit + nwarps;
+    uint64_t lo_n = 0, hi_n = 0;
+    if (un < n_units && r0 + un * 32 + lane < r1) {
+      lo_n = __ldcs(off + r0 + un * 32 + lane);
+      hi_n = __ldcs(off + r0 + un * 32 + lane + 1);
     }
-    s += __shfl_xor_sync(0xffffffffu, s, 4);
-    s += __shfl_xor_sync(0xffffffffu, s, 2);
-    s += __shfl_xor_sync(0xffffffffu, s, 1);
-    if (valid && sub == 0) dl += upd.apply(v, s);
+    const bool mine = row0 + lane < r1;
+    const typename Update::operands ops = upd.load(mine ? row0 + lane : row0);
+    const uint64_t base = __shfl_sync(0xffffffffu, lo, 0);
+    const uint32_t sb = mine ? static_cast<uint32_t>(lo - base) : 0u;
+    const uint32_t se = mine ? static_cast<uint32_t>(hi - base) : 0u;
+    const uint32_t* ab = adj + base;
+    uint32_t b = __shfl_sync(0xffffffffu, sb, slot), e = __shfl_sync(0xffffffffu, se, slot);
+    row_ids<LPR> cur;
+    cur.load(ab, b + q, e);
+    float res = 0.f;
+#pragma unroll 1
+    for (uint32_t t = 0; t < LPR; ++t) {  // 32 rows / RPR rows per round = LPR rounds
+      uint32_t bn = 0, en = 0;
+      row_ids<LPR> nxt{0u, 0u, 0u, 0u};
+      if (t + 1 < LPR) {
+        bn = __shfl_sync(0xffffffffu, sb, (t + 1) * RPR + slot);
+        en = __shfl_sync(0xffffffffu, se, (t + 1) * RPR + slot);
+        nxt.load(ab, bn + q, en);
+      }
+      const uint32_t j = b + q;
+      const float g0 = j < e ? __ldg(x + cur.a0) : 0.f;
+      const float g1 = j + LPR < e ? __ldg(x + cur.a1) : 0.f;
+      const float g2 = j + 2 * LPR < e ? __ldg(x + cur.a2) : 0.f;
+      const float g3 = j + 3 * LPR < e ? __ldg(x + cur.a3) : 0.f;
+      float s = (g0 + g1) + (g2 + g3);
+#pragma unroll
+      for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      // row t*RPR + k sits in lanes k*LPR..; lane L collects row L in round L / RPR
+      const float v = __shfl_sync(0xffffffffu, s, (lane % RPR) * LPR);
+      if (lane / RPR == t) res = v;
+      cur = nxt;
+      b = bn;
+      e = en;
+    }
+    if (mine) dl += upd.apply(row0 + lane, res, ops);
+    lo = lo_n;
+    hi = hi_n;
   }
   dl = block_sum<256>(dl, s_red);
   if (threadIdx.x == 0) partials[blockIdx.x] = dl;
@@ -212,7 +267,7 @@ __global__ void __launch_bounds__(256) k_pull_short(pull_plan_view pv, const uin
                                                     double* __restrict__ partials) {
   __shared__ double s_red[32];
   if (upd.skip()) return;
-  const uint32_t base = pv.n_long + pv.n_mid;
+  const uint32_t base = pv.short_begin;
   double dl = 0.0;
   for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; base + r < pv.V;
        r += (uint64_t)gridDim.x * blockDim.x) {

@@ -54,14 +54,29 @@ struct rank_update {
 
   __device__ __forceinline__ bool skip() const { return mode && *mode == 2; }
 
-  __device__ __forceinline__ double apply(uint32_t v, float y) const {
+  __device__ __forceinline__ bool storing_rank() const { return mode ? (*mode == 1) : (final_epoch != 0); }
+
+  // The inputs of apply() that do not depend on the gathered sum; a kernel
+  // may load them before its gathers so that their latency overlaps.
+  struct operands {
+    uint32_t dg;
+    float xo;
+  };
+  __device__ __forceinline__ operands load(uint32_t v) const {
+    if (storing_rank()) return {0u, 0.f};
+    return {__ldcs(deg + v), __ldcs(x + v)};
+  }
+
+  __device__ __forceinline__ double apply(uint32_t v, float y) const { return apply(v, y, load(v)); }
+
+  __device__ __forceinline__ double apply(uint32_t v, float y, operands o) const {
     const float r = fmaf(d, y, tele(v));
-    if (mode ? (*mode == 1) : (final_epoch != 0)) {
+    if (storing_rank()) {
       xn[v] = r;
       return 0.0;
     }
-    const uint32_t dg = __ldcs(deg + v);
-    const float xo = __ldcs(x + v);
+    const uint32_t dg = o.dg;
+    const float xo = o.xo;
     float xv, dl;
     if (dg > 0) {
       const float fd = static_cast<float>(dg);

@@ -25,12 +25,15 @@ namespace plato_b200 {
 // Degree-bin plan of a relabelled graph (see pull_binned.cuh).
 struct pull_plan {
   bool valid = false;
-  uint32_t n_long = 0, n_mid = 0, n_items = 0, n_hubs = 0;
-  uint32_t blocks_long = 0, blocks_hubs = 0, blocks_mid = 0, blocks_short = 0;
+  uint32_t n_long = 0, n_items = 0, n_hubs = 0;
+  uint32_t rows_begin[4] = {0, 0, 0, 0};  // k_pull_rows<16>, <8>, <4> bins; [3] = first short row
+  uint32_t blocks_long = 0, blocks_hubs = 0, blocks_rows[3] = {0, 0, 0}, blocks_short = 0;
   dbuf<uint2> items;
   dbuf<uint32_t> hub_rows, hub_item0, hub_pieces;
   dbuf<float> piece_sum;
-  uint32_t partials() const { return blocks_long + blocks_hubs + blocks_mid + blocks_short; }
+  uint32_t partials() const {
+    return blocks_long + blocks_hubs + blocks_rows[0] + blocks_rows[1] + blocks_rows[2] + blocks_short;
+  }
 };
 
 struct rank_workspace {
@@ -98,9 +101,15 @@ int build_plan(plato_graph* g, pull_plan& pl, cudaStream_t st) {
   PLATO_CUDA_TRY(cudaStreamSynchronize(st));
   for (uint32_t v = 1; v < V; ++v)
     if (deg[v] > deg[v - 1]) return PLATO_OK;  // not sorted: keep the merge-path kernel
-  uint32_t n_long = 0, n_mid = 0;
-  while (n_long < V && deg[n_long] > kMidMax) ++n_long;
-  while (n_long + n_mid < V && deg[n_long + n_mid] > kShortMax) ++n_mid;
+  uint32_t n_long = 0;
+  while (n_long < V && deg[n_long] > kRowsMax[0]) ++n_long;
+  uint32_t row = n_long;
+  for (int b = 0; b < 3; ++b) {
+    pl.rows_begin[b] = row;
+    const uint32_t lower = b < 2 ? kRowsMax[b + 1] : kShortMax;
+    while (row < V && deg[row] > lower) ++row;
+  }
+  pl.rows_begin[3] = row;
   // long-bin units: the pieces of every hub row, then groups of consecutive
   // rows (up to kGroupRows rows and kGroupEdges edges, at least one row)
   std::vector<uint2> items;
@@ -126,7 +135,6 @@ int build_plan(plato_graph* g, pull_plan& pl, cudaStream_t st) {
     r += n;
   }
   pl.n_long = n_long;
-  pl.n_mid = n_mid;
   pl.n_items = static_cast<uint32_t>(items.size());
   pl.n_hubs = static_cast<uint32_t>(hr.size());
   PLATO_TRY(pl.items.alloc(std::max<size_t>(items.size(), 1)));
@@ -142,7 +150,7 @@ int build_plan(plato_graph* g, pull_plan& pl, cudaStream_t st) {
     PLATO_CUDA_TRY(cudaMemcpyAsync(pl.hub_pieces.p, hp.data(), hp.size() * 4, cudaMemcpyHostToDevice, st));
   }
   PLATO_CUDA_TRY(cudaStreamSynchronize(st));
-  const uint64_t n_short = static_cast<uint64_t>(V) - n_long - n_mid;
+  const uint64_t n_short = static_cast<uint64_t>(V) - pl.rows_begin[3];
   // fixed grids of up to 8 CTAs (64 warps) per SM; the kernels stride over their work
   int sms = 0;
   PLATO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
@@ -151,8 +159,9 @@ int build_plan(plato_graph* g, pull_plan& pl, cudaStream_t st) {
     return static_cast<uint32_t>(std::min<uint64_t>((threads + 255) / 256, cap));
   };
   pl.blocks_long = blocks(static_cast<uint64_t>(pl.n_items) * 32);
-  pl.blocks_hubs = blocks(pl.n_hubs);
-  pl.blocks_mid = blocks(static_cast<uint64_t>(n_mid) * 8);
+  pl.blocks_hubs = blocks(static_cast<uint64_t>(pl.n_hubs) * 32);
+  for (int b = 0; b < 3; ++b)  // one warp per 32 rows
+    pl.blocks_rows[b] = blocks(static_cast<uint64_t>(pl.rows_begin[b + 1] - pl.rows_begin[b] + 31) / 32 * 32);
   pl.blocks_short = blocks(n_short);
   pl.valid = true;
   return PLATO_OK;
@@ -229,7 +238,7 @@ int pull_epoch(plato_graph* g, const float* x, float* xn, Tele tele, float d, bo
   rank_update<Tele> upd{x, xn, g->out_deg.p, tele, d, final_epoch ? 1 : 0, mode};
   const pull_plan& pl = ws->plan;
   if (pl.valid) {
-    const pull_plan_view pv{pl.n_long, pl.n_mid, g->info.vertices, pl.n_items, pl.items.p,
+    const pull_plan_view pv{pl.n_long, pl.rows_begin[3], g->info.vertices, pl.n_items, pl.items.p,
                             pl.n_hubs, pl.hub_rows.p, pl.hub_item0.p, pl.hub_pieces.p,
                             pl.piece_sum.p};
     double* part = ws->partials.p;
@@ -245,12 +254,27 @@ int pull_epoch(plato_graph* g, const float* x, float* xn, Tele tele, float d, bo
       PLATO_LAUNCHED("k_pull_hubs");
     }
     part += pl.blocks_hubs;
-    if (pl.blocks_mid) {
-      prof_scope ps("k_pull_mid", st);
-      k_pull_mid<rank_update<Tele>><<<pl.blocks_mid, 256, 0, st>>>(pv, g->in_off.p, g->in_adj.p, x, upd, part);
-      PLATO_LAUNCHED("k_pull_mid");
+    if (pl.blocks_rows[0]) {
+      prof_scope ps("k_pull_rows16", st);
+      k_pull_rows<16, rank_update<Tele>><<<pl.blocks_rows[0], 256, 0, st>>>(
+          pl.rows_begin[0], pl.rows_begin[1], g->in_off.p, g->in_adj.p, x, upd, part);
+      PLATO_LAUNCHED("k_pull_rows16");
     }
-    part += pl.blocks_mid;
+    part += pl.blocks_rows[0];
+    if (pl.blocks_rows[1]) {
+      prof_scope ps("k_pull_rows8", st);
+      k_pull_rows<8, rank_update<Tele>><<<pl.blocks_rows[1], 256, 0, st>>>(
+          pl.rows_begin[1], pl.rows_begin[2], g->in_off.p, g->in_adj.p, x, upd, part);
+      PLATO_LAUNCHED("k_pull_rows8");
+    }
+    part += pl.blocks_rows[1];
+    if (pl.blocks_rows[2]) {
+      prof_scope ps("k_pull_rows4", st);
+      k_pull_rows<4, rank_update<Tele>><<<pl.blocks_rows[2], 256, 0, st>>>(
+          pl.rows_begin[2], pl.rows_begin[3], g->in_off.p, g->in_adj.p, x, upd, part);
+      PLATO_LAUNCHED("k_pull_rows4");
+    }
+    part += pl.blocks_rows[2];
     if (pl.blocks_short) {
       prof_scope ps("k_pull_short", st);
       k_pull_short<rank_update<Tele>><<<pl.blocks_short, 256, 0, st>>>(pv, g->in_off.p, g->in_adj.p, x, upd, part);
