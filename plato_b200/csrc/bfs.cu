@@ -10,6 +10,12 @@
 //   that is in the current frontier.
 // A vertex first reached in epoch e has level e + 1 (root: 0).  Levels are
 // unique; parents depend on claim order in push mode, as in the reference.
+//
+// One kernel launch per level (k_bfs_level): it runs the push or the pull
+// step that the previous level chose, clears the frontier buffer that the
+// level after next fills, and its last CTA to finish counts the new frontier
+// and chooses the next level's mode (no CTA waits for another).
+#include <algorithm>
 #include <new>
 
 #include "graph.cuh"
@@ -25,10 +31,11 @@ struct bfs_control {
   uint32_t pushes;           // of which push
   unsigned long long visited;
   unsigned long long trace;  // bit i: level i ran push (first 64 levels)
+  unsigned int arrived;      // CTAs of the running level that finished
 };
 
 struct bfs_workspace {
-  push_frontier fr[2];
+  push_frontier fr[3];  // current, next, and the one cleared for the level after
   dbuf<uint32_t> visited;
   dbuf<uint32_t> level, parent;
   dbuf<bfs_control> ctrl;
@@ -41,23 +48,6 @@ struct bfs_workspace {
 void destroy_bfs_workspace(bfs_workspace* ws) { delete ws; }
 
 namespace {
-
-// After a level: count it, fold the new frontier into the visited count and
-// pick the next level's mode from its active-edge count (dualmode.hpp:264-279).
-__global__ void k_bfs_control(frontier_view fn, bfs_control* c, double edges, double threshold) {
-  if (threadIdx.x != 0 || c->done) return;
-  const unsigned long long actives = fn.counters[0];
-  if (c->mode == 1) c->pushes += 1;
-  c->level += 1;
-  c->visited += actives;
-  if (actives == 0) {
-    c->done = 1;
-    return;
-  }
-  const int push = (static_cast<double>(fn.counters[2]) / edges) < threshold ? 1 : 0;
-  c->mode = push;
-  if (push && c->level < 64) c->trace |= 1ull << c->level;
-}
 
 __global__ void k_bfs_init(uint32_t V, uint32_t root, uint32_t invalid_parent, uint32_t* level,
                            uint32_t* parent, uint32_t* visited) {
@@ -73,85 +63,157 @@ __global__ void k_bfs_init(uint32_t V, uint32_t root, uint32_t invalid_parent, u
   }
 }
 
-// Push level: frontier chunks -> claim unvisited out-neighbours.
-__global__ void __launch_bounds__(256) k_bfs_push(frontier_view cur, frontier_view next,
-                                                  const uint64_t* __restrict__ out_off,
-                                                  const uint32_t* __restrict__ out_adj,
-                                                  const uint32_t* __restrict__ deg,
-                                                  uint32_t* visited, uint32_t* level,
-                                                  uint32_t* parent, uint32_t new_level,
-                                                  const bfs_control* ctrl) {
-  if (ctrl->done || ctrl->mode != 1) return;  // uniform: pull level or finished
-  const unsigned long long nchunks = cur.counters[1];
+struct bfs_level_args {
+  frontier_view cur, next, spare;
+  uint32_t V;
+  const uint64_t* __restrict__ out_off;
+  const uint32_t* __restrict__ out_adj;
+  const uint32_t* __restrict__ out_deg;
+  const uint64_t* __restrict__ in_off;
+  const uint32_t* __restrict__ in_adj;
+  uint32_t* visited;
+  uint32_t* level;
+  uint32_t* parent;
+  uint32_t new_level;
+  bfs_control* ctrl;
+  double edges, threshold;
+};
+
+__device__ __forceinline__ void bfs_visit(const bfs_level_args& a, uint32_t v, uint32_t par) {
+  a.level[v] = a.new_level;
+  a.parent[v] = par;
+  const uint32_t bit = 1u << (v & 31);
+  atomicOr(&a.visited[v >> 5], bit);
+  atomicOr(&a.next.bits[v >> 5], bit);
+}
+
+// Push step: frontier chunks -> claim unvisited out-neighbours.
+__device__ __forceinline__ void bfs_push_step(const bfs_level_args& a) {
+  const unsigned long long nchunks = a.cur.counters[1];
   const unsigned lane = threadIdx.x & 31;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   for (uint64_t c = warp; c < nchunks; c += nwarps) {
-    const uint2 ch = cur.chunks[c];
+    const uint2 ch = a.cur.chunks[c];
     const uint32_t u = ch.x;
-    const uint64_t b = out_off[u] + static_cast<uint64_t>(ch.y) * kPushChunk;
-    const uint64_t e_end = min(b + kPushChunk, out_off[u + 1]);
+    const uint64_t b = a.out_off[u] + static_cast<uint64_t>(ch.y) * kPushChunk;
+    const uint64_t e_end = min(b + kPushChunk, a.out_off[u + 1]);
     for (uint64_t base = b; base < e_end; base += 32) {
       const uint64_t e = base + lane;
       uint32_t dst = 0;
       bool fresh = false;
       if (e < e_end) {
-        dst = out_adj[e];
+        dst = a.out_adj[e];
         const uint32_t bit = 1u << (dst & 31);
-        if (!(visited[dst >> 5] & bit)) fresh = !(atomicOr(&visited[dst >> 5], bit) & bit);
+        if (!(a.visited[dst >> 5] & bit)) fresh = !(atomicOr(&a.visited[dst >> 5], bit) & bit);
         if (fresh) {
-          level[dst] = new_level;
-          parent[dst] = u;
-          atomicOr(&next.bits[dst >> 5], bit);
+          a.level[dst] = a.new_level;
+          a.parent[dst] = u;
+          atomicOr(&a.next.bits[dst >> 5], bit);
         }
       }
-      frontier_append_warp(next, fresh, dst, deg);
+      frontier_append_warp(a.next, fresh, dst, a.out_deg);
     }
   }
 }
 
-// Pull level: every unvisited vertex scans its in-edges for a frontier member.
-__global__ void __launch_bounds__(256) k_bfs_pull(uint32_t V, frontier_view cur, frontier_view next,
-                                                  const uint64_t* __restrict__ in_off,
-                                                  const uint32_t* __restrict__ in_adj,
-                                                  const uint32_t* __restrict__ deg,
-                                                  uint32_t* visited, uint32_t* level,
-                                                  uint32_t* parent, uint32_t new_level,
-                                                  const bfs_control* ctrl) {
-  if (ctrl->done || ctrl->mode != 0) return;  // uniform: push level or finished
+// Pull step: every unvisited vertex takes the first in-neighbour (CSC order)
+// that is in the current frontier.  A thread per row tests the row's first
+// four in-edges (all ids, then all bitmap probes, in flight together); most
+// rows of a pull level stop there.  The rows still open are finished by
+// their warp, one row at a time, in rounds of 32 in-edges whose first hit is
+// found with a ballot, so the parent equals that of a one-by-one scan.
+__device__ __forceinline__ void bfs_pull_step(const bfs_level_args& a) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t* cur = a.cur.bits;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  const uint64_t nrounds = (V + stride - 1) / stride;
-  for (uint64_t r = 0; r < nrounds; ++r) {  // warp-uniform trip count for the appends
-    const uint64_t v = r * stride + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    bool fresh = false;
-    if (v < V && !test_bit(visited, static_cast<uint32_t>(v))) {
-      const uint64_t b = in_off[v], e = in_off[v + 1];
-      // four in-neighbours per step (ids, then bitmap tests, all in flight);
-      // the first hit in CSC order is the parent, as in a one-by-one scan
-      for (uint64_t i = b; i < e; i += 4) {
-        const bool p1 = i + 1 < e, p2 = i + 2 < e, p3 = i + 3 < e;
-        const uint32_t s0 = in_adj[i];
-        const uint32_t s1 = p1 ? in_adj[i + 1] : 0u;
-        const uint32_t s2 = p2 ? in_adj[i + 2] : 0u;
-        const uint32_t s3 = p3 ? in_adj[i + 3] : 0u;
-        const bool h0 = test_bit(cur.bits, s0);
-        const bool h1 = p1 && test_bit(cur.bits, s1);
-        const bool h2 = p2 && test_bit(cur.bits, s2);
-        const bool h3 = p3 && test_bit(cur.bits, s3);
-        if (h0 || h1 || h2 || h3) {
-          const uint32_t s = h0 ? s0 : h1 ? s1 : h2 ? s2 : s3;
-          fresh = true;
-          level[v] = new_level;
-          parent[v] = s;
-          const uint32_t bit = 1u << (v & 31);
-          atomicOr(&visited[v >> 5], bit);
-          atomicOr(&next.bits[v >> 5], bit);
+  const uint64_t rounds = (a.V + stride - 1) / stride;
+  for (uint64_t r = 0; r < rounds; ++r) {  // warp-uniform trip count
+    const uint64_t v64 = r * stride + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint32_t v = static_cast<uint32_t>(v64);
+    bool found = false, open = false;
+    uint32_t par = 0;
+    uint64_t next_edge = 0, e = 0;
+    if (v64 < a.V && !test_bit(a.visited, v)) {
+      const uint64_t b = a.in_off[v];
+      e = a.in_off[v + 1];
+      const bool p0 = b < e, p1 = b + 1 < e, p2 = b + 2 < e, p3 = b + 3 < e;
+      const uint32_t s0 = p0 ? a.in_adj[b] : 0u;
+      const uint32_t s1 = p1 ? a.in_adj[b + 1] : 0u;
+      const uint32_t s2 = p2 ? a.in_adj[b + 2] : 0u;
+      const uint32_t s3 = p3 ? a.in_adj[b + 3] : 0u;
+      const bool h0 = p0 && test_bit(cur, s0);
+      const bool h1 = p1 && test_bit(cur, s1);
+      const bool h2 = p2 && test_bit(cur, s2);
+      const bool h3 = p3 && test_bit(cur, s3);
+      found = h0 || h1 || h2 || h3;
+      par = h0 ? s0 : h1 ? s1 : h2 ? s2 : s3;
+      next_edge = b + 4;
+      open = !found && next_edge < e;
+    }
+    unsigned todo = __ballot_sync(0xffffffffu, open);
+    while (todo) {  // warp-uniform
+      const int l = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const uint64_t rb = __shfl_sync(0xffffffffu, next_edge, l);
+      const uint64_t re = __shfl_sync(0xffffffffu, e, l);
+      for (uint64_t i = rb + lane; i - lane < re; i += 32) {
+        const uint32_t sv = i < re ? a.in_adj[i] : 0u;
+        const unsigned hit = __ballot_sync(0xffffffffu, i < re && test_bit(cur, sv));
+        if (hit) {
+          const uint32_t p = __shfl_sync(0xffffffffu, sv, __ffs(hit) - 1);
+          if (lane == static_cast<unsigned>(l)) {
+            found = true;
+            par = p;
+          }
           break;
         }
       }
     }
-    frontier_append_warp(next, fresh, static_cast<uint32_t>(v), deg);
+    if (found) bfs_visit(a, v, par);
+    frontier_append_warp(a.next, found, v, a.out_deg);
   }
+}
+
+__global__ void __launch_bounds__(256) k_bfs_level(bfs_level_args a) {
+  __shared__ bool s_last;
+  bfs_control* c = a.ctrl;
+  if (c->done) return;  // uniform: the search ended at an earlier level
+  const int mode = c->mode;
+  // the level after next writes into `spare`; nothing reads it in this level
+  const uint32_t words = (a.V + 31) / 32;
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += gridDim.x * blockDim.x)
+    a.spare.bits[w] = 0;
+  if (blockIdx.x == 0 && threadIdx.x < 3) a.spare.counters[threadIdx.x] = 0;
+
+  if (mode == 1)
+    bfs_push_step(a);
+  else
+    bfs_pull_step(a);
+
+  // the last CTA to finish sees every append (fence + ticket) and decides
+  // the next level (dualmode.hpp:264-279; bfs.hpp:92 ends on no activation)
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&c->arrived, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last || threadIdx.x != 0) return;
+  __threadfence();
+  c->arrived = 0;
+  const unsigned long long actives = atomicAdd(&a.next.counters[0], 0ull);
+  const unsigned long long active_edges = atomicAdd(&a.next.counters[2], 0ull);
+  if (mode == 1) c->pushes += 1;
+  c->level += 1;
+  c->visited += actives;
+  if (actives == 0) {
+    c->done = 1;
+    return;
+  }
+  const int push = (static_cast<double>(active_edges) / a.edges) < a.threshold ? 1 : 0;
+  c->mode = push;
+  if (push && c->level < 64) c->trace |= 1ull << c->level;
 }
 
 int ensure_bfs_ws(plato_graph* g) {
@@ -161,8 +223,7 @@ int ensure_bfs_ws(plato_graph* g) {
   }
   bfs_workspace* ws = g->bfs_ws;
   const uint32_t V = g->info.vertices;
-  PLATO_TRY(frontier_alloc(ws->fr[0], g));
-  PLATO_TRY(frontier_alloc(ws->fr[1], g));
+  for (push_frontier& f : ws->fr) PLATO_TRY(frontier_alloc(f, g));
   PLATO_TRY(ws->visited.alloc((V + 31) / 32));
   PLATO_TRY(ws->level.alloc(V));
   PLATO_TRY(ws->parent.alloc(V));
@@ -197,42 +258,50 @@ int bfs_impl(plato_graph* g, const plato_bfs_opts* o, const plato_dualmode_opts*
                                                 ws->visited.p);
   PLATO_LAUNCHED("k_bfs_init");
   PLATO_TRY(frontier_reset(ws->fr[0], V, st));
+  PLATO_TRY(frontier_reset(ws->fr[1], V, st));
   PLATO_TRY(frontier_seed(ws->fr[0], g, root, st));
   PLATO_TRY(frontier_read(ws->fr[0], st));
 
-  // Level loop with the engine switch on the device: after each level
-  // k_bfs_control reads the new frontier's counters, decides push or pull for
-  // the next level (dualmode.hpp:264-279) and flags the end (bfs.hpp:92, no
-  // vertex activated).  The host enqueues levels in batches and polls between
-  // batches; levels enqueued after the end return at once.
+  // Level loop with the engine switch on the device (k_bfs_level).  The host
+  // enqueues levels in batches and polls between batches; levels enqueued
+  // after the end return at once.
   const double edges = static_cast<double>(g->stored_edges);
   const bool first_push = (static_cast<double>(ws->fr[0].h_counters[2]) / edges) < threshold;
-  const bfs_control init{first_push ? 1 : 0, 0, 0, 0, 1ull, first_push ? 1ull : 0ull};
+  const bfs_control init{first_push ? 1 : 0, 0, 0, 0, 1ull, first_push ? 1ull : 0ull, 0u};
   PLATO_CUDA_TRY(cudaMemcpyAsync(ws->ctrl.p, &init, sizeof(init), cudaMemcpyHostToDevice, st));
-  const unsigned push_blocks = 148 * 16;
-  const unsigned pull_blocks = grid_for(V, 256, 148 * 8);
-  constexpr uint32_t kBatch = 4;
+  // one full wave of resident CTAs; the steps stride over their work
+  int sms = 0, per_sm = 0;
+  PLATO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
+  PLATO_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bfs_level, 256, 0));
+  const unsigned blocks = static_cast<unsigned>(sms) * static_cast<unsigned>(std::max(per_sm, 1));
+  bfs_level_args a{};
+  a.V = V;
+  a.out_off = g->out_off.p;
+  a.out_adj = g->out_adj.p;
+  a.out_deg = g->out_deg.p;
+  a.in_off = g->in_off.p;
+  a.in_adj = g->in_adj.p;
+  a.visited = ws->visited.p;
+  a.level = ws->level.p;
+  a.parent = ws->parent.p;
+  a.ctrl = ws->ctrl.p;
+  a.edges = edges;
+  a.threshold = threshold;
   uint32_t launched = 0;
+  uint32_t batch = 8;  // RMAT searches end within about 8 levels
   for (;;) {
-    for (uint32_t k = 0; k < kBatch; ++k, ++launched) {
-      const int cur = static_cast<int>(launched & 1u);
-      push_frontier& fc = ws->fr[cur];
-      push_frontier& fn = ws->fr[cur ^ 1];
-      PLATO_TRY(frontier_reset(fn, V, st));
-      k_bfs_push<<<push_blocks, 256, 0, st>>>(fc.view(), fn.view(), g->out_off.p, g->out_adj.p,
-                                              g->out_deg.p, ws->visited.p, ws->level.p,
-                                              ws->parent.p, launched + 1, ws->ctrl.p);
-      PLATO_LAUNCHED("k_bfs_push");
-      k_bfs_pull<<<pull_blocks, 256, 0, st>>>(V, fc.view(), fn.view(), g->in_off.p, g->in_adj.p,
-                                              g->out_deg.p, ws->visited.p, ws->level.p,
-                                              ws->parent.p, launched + 1, ws->ctrl.p);
-      PLATO_LAUNCHED("k_bfs_pull");
-      k_bfs_control<<<1, 32, 0, st>>>(fn.view(), ws->ctrl.p, edges, threshold);
-      PLATO_LAUNCHED("k_bfs_control");
+    for (uint32_t k = 0; k < batch; ++k, ++launched) {
+      a.cur = ws->fr[launched % 3].view();
+      a.next = ws->fr[(launched + 1) % 3].view();
+      a.spare = ws->fr[(launched + 2) % 3].view();
+      a.new_level = launched + 1;
+      k_bfs_level<<<blocks, 256, 0, st>>>(a);
+      PLATO_LAUNCHED("k_bfs_level");
     }
     PLATO_CUDA_TRY(cudaMemcpyAsync(ws->h_ctrl, ws->ctrl.p, sizeof(bfs_control), cudaMemcpyDeviceToHost, st));
     PLATO_CUDA_TRY(cudaStreamSynchronize(st));
     if (ws->h_ctrl->done) break;
+    batch = 4;
   }
   const bfs_control& c = *ws->h_ctrl;
   if (stats) {

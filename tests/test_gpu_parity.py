@@ -164,6 +164,37 @@ def test_bfs_push_only_and_pull_only(rmat14_sym):
             assert st.push_iterations == (st.iterations if thr > 1 else 0)
 
 
+@pytest.mark.parametrize("relabel", [True, False])
+def test_bfs_pull_parent_is_first_frontier_in_neighbour(rmat14_sym, relabel):
+    """Pull levels take the first in-neighbour in CSC order that is in the
+    frontier (bfs.hpp:119-136).  Without relabelling CSC order is ascending
+    caller id, so the parent is the smallest in-neighbour one level up; with
+    relabelling the warp, 8-lane and thread rows must still give exact levels
+    and valid parents."""
+    V, s, d, _ = rmat14_sym
+    deg = np.bincount(s, minlength=V) + np.bincount(d, minlength=V)
+    roots = np.random.default_rng(5).choice(np.flatnonzero(deg > 0), 3, replace=False)
+    u = np.concatenate([s, d]).astype(np.int64)
+    v = np.concatenate([d, s]).astype(np.int64)
+    with pb.Graph(V, s, d, False, relabel=relabel) as g:
+        for root in roots:
+            lev_ref = fp64.bfs_levels(V, s, d, int(root), False)
+            lev, par, st = g.bfs(int(root), push_threshold=0.0)
+            np.testing.assert_array_equal(lev, lev_ref)
+            assert st.push_iterations == 0
+            reached = np.flatnonzero((lev != pb.PLATO_LEVEL_UNREACHED) & (np.arange(V) != root))
+            lv = lev.astype(np.int64)
+            ok = (lev[u] != pb.PLATO_LEVEL_UNREACHED) & (lv[u] == lv[v] - 1)
+            first = np.full(V, V, np.int64)
+            np.minimum.at(first, v[ok], u[ok])
+            if relabel:
+                assert (lev[par[reached]] == lev[reached] - 1).all()
+                key = par[reached].astype(np.int64) * V + reached
+                assert np.isin(key, u * V + v).all()
+            else:
+                np.testing.assert_array_equal(par[reached], first[reached])
+
+
 def test_bfs_isolated_root_and_edge_cases():
     # vertex 3 has no edges; graph of 5 vertices with a small chain
     s = np.array([0, 1], np.uint32)
