@@ -208,30 +208,27 @@ __global__ void __launch_bounds__(256, 5) k_batch_pull(batch_pass p0) {
   int jj = ja;
   for (int r = ra; r <= rb; ++r) {
     const int e_end = (r < rb) ? static_cast<int>(s_rowend[r]) : jb;
-    for (; jj + 8 <= e_end; jj += 8) {  // eight row gathers in flight per lane
+    // rounds of eight row gathers in flight per lane; the last round of a
+    // row is predicated instead of a serial tail, so a row costs one gather
+    // latency per eight in-edges
+    for (; jj < e_end; jj += 8) {
+      const int n = e_end - jj;
       float a[8][VEC];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) ldvec<VEC>(xl + static_cast<size_t>(s_src[jj + u]) * KT, a[u]);
+      for (int u = 0; u < 8; ++u) {
+        if (u < n) {
+          ldvec<VEC>(xl + static_cast<size_t>(s_src[jj + u]) * KT, a[u]);
+        } else {
+#pragma unroll
+          for (int c = 0; c < VEC; ++c) a[u][c] = 0.f;
+        }
+      }
 #pragma unroll
       for (int c = 0; c < VEC; ++c)
         acc[c] += ((a[0][c] + a[1][c]) + (a[2][c] + a[3][c])) +
                   ((a[4][c] + a[5][c]) + (a[6][c] + a[7][c]));
     }
-    for (; jj + 4 <= e_end; jj += 4) {
-      float a0[VEC], a1[VEC], a2[VEC], a3[VEC];
-      ldvec<VEC>(xl + static_cast<size_t>(s_src[jj]) * KT, a0);
-      ldvec<VEC>(xl + static_cast<size_t>(s_src[jj + 1]) * KT, a1);
-      ldvec<VEC>(xl + static_cast<size_t>(s_src[jj + 2]) * KT, a2);
-      ldvec<VEC>(xl + static_cast<size_t>(s_src[jj + 3]) * KT, a3);
-#pragma unroll
-      for (int c = 0; c < VEC; ++c) acc[c] += (a0[c] + a1[c]) + (a2[c] + a3[c]);
-    }
-    for (; jj < e_end; ++jj) {
-      float a0[VEC];
-      ldvec<VEC>(xl + static_cast<size_t>(s_src[jj]) * KT, a0);
-#pragma unroll
-      for (int c = 0; c < VEC; ++c) acc[c] += a0[c];
-    }
+    jj = e_end;  // the last round may step past the row's end
     if (r < rb) {
       if (r == head) {
         head_done = true;
