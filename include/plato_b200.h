@@ -262,10 +262,37 @@ typedef struct {
 typedef struct plato_edge_list plato_edge_list;
 int plato_rmat_generate(const plato_rmat_params* p, plato_edge_list** out);
 int plato_edge_list_info(const plato_edge_list* el, plato_vid_t* vertices, uint64_t* edges);
-/* Pointers stay valid until plato_edge_list_free. Edges are sorted by (src, dst). */
+/* Pointers stay valid until plato_edge_list_free.  RMAT lists are sorted by
+ * (src, dst); lists read from files keep file order. */
 int plato_edge_list_data(const plato_edge_list* el, const plato_vid_t** src,
                          const plato_vid_t** dst);
 int plato_edge_list_free(plato_edge_list* el);
+
+/* ---- files ------------------------------------------------------------------
+ * Edge list from CSV text.  Replaces load_edges_cache + csv_parser
+ * (plato/graph/structure.hpp:190-237, plato/graph/parsers.hpp:226-290,
+ * plato/graph/detail.hpp:82-108, 196-212):
+ *   path   one file, or a directory whose regular files are read in name
+ *          order; names ending in ".gz" are gzip-compressed;
+ *   lines  "src,dst": fields split at commas (empty fields skipped), each id
+ *          read as strtoul(field, 10) reads it; empty lines and lines without
+ *          a destination are skipped; an id above 2^32-1 -> PLATO_EINVAL
+ *          (the reference aborts);
+ *   info   edges = lines parsed, vertices = largest id + 1 (the reference's
+ *          distinct-id count on the compact ids it requires).
+ * The result feeds plato_graph_create like an RMAT list. */
+int plato_edge_list_read_csv(const char* path, plato_edge_list** out);
+
+/* Per-vertex results as CSV, the layout the reference's examples write
+ * (example/pagerank.cc:191-200, plato/util/foutput.cc:95-101):
+ * `files` files <dir>/<prefix><NNNN>.csv (".csv.gz" when gzip != 0), each
+ * holding a contiguous vertex range, one "v,value" line per vertex; float
+ * values printed as %g (ostream's default for double), uint32 values as
+ * integers.  `values` is host memory indexed by caller vertex id. */
+#define PLATO_VALUE_F32 0
+#define PLATO_VALUE_U32 1
+int plato_write_vertex_csv(const char* dir, const char* prefix, const void* values,
+                           int value_type, uint32_t n, uint32_t files, int gzip);
 
 #ifdef __cplusplus
 }  /* extern "C" */

@@ -19,6 +19,7 @@ Every call runs the CUDA kernels of libplato_b200.so; there is no CPU path.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -28,7 +29,7 @@ from ._lib import (PLATO_GRAPH_RELABEL, PLATO_LEVEL_UNREACHED, PLATO_PPR_PULL, P
                    PlatoError, check, load)
 
 __all__ = [
-    "Graph", "GraphInfo", "PlatoError", "rmat", "pagerank", "personalized_pagerank",
+    "Graph", "GraphInfo", "PlatoError", "rmat", "read_csv", "write_vertex_csv", "pagerank", "personalized_pagerank",
     "breadth_first_search", "pagerank_opts_t", "personalized_pagerank_opts_t", "bfs_opts_t",
     "dualmode_engine_opts_t", "PLATO_LEVEL_UNREACHED", "PLATO_PPR_PULL", "PLATO_PPR_PUSHPULL",
     "kernel_launches",
@@ -98,16 +99,8 @@ def _ptr(a: np.ndarray) -> C.c_void_p:
     return C.c_void_p(a.ctypes.data)
 
 
-def rmat(scale: int, edgefactor: int = 16, seed: int = 1, a: float = 0.57, b: float = 0.19,
-         c: float = 0.19, symmetrize: bool = False, permute: bool = False):
-    """Seeded RMAT edge list -> (V, src, dst) numpy uint32 arrays sorted by (src, dst).
-
-    Self-loops and duplicates removed, ids compacted to [0, V); symmetrised
-    graphs keep one (min, max) entry per unordered pair."""
-    lib = load()
-    p = _lib.RmatParams(scale, edgefactor, seed, a, b, c, int(symmetrize), int(permute))
-    h = C.c_void_p()
-    check(lib.plato_rmat_generate(C.byref(p), C.byref(h)), "plato_rmat_generate")
+def _take_edge_list(lib, h):
+    """Copies an edge-list handle into numpy arrays and frees it."""
     try:
         V = C.c_uint32()
         E = C.c_uint64()
@@ -123,6 +116,44 @@ def rmat(scale: int, edgefactor: int = 16, seed: int = 1, a: float = 0.57, b: fl
         return int(V.value), src, dst
     finally:
         lib.plato_edge_list_free(h)
+
+
+def rmat(scale: int, edgefactor: int = 16, seed: int = 1, a: float = 0.57, b: float = 0.19,
+         c: float = 0.19, symmetrize: bool = False, permute: bool = False):
+    """Seeded RMAT edge list -> (V, src, dst) numpy uint32 arrays sorted by (src, dst).
+
+    Self-loops and duplicates removed, ids compacted to [0, V); symmetrised
+    graphs keep one (min, max) entry per unordered pair."""
+    lib = load()
+    p = _lib.RmatParams(scale, edgefactor, seed, a, b, c, int(symmetrize), int(permute))
+    h = C.c_void_p()
+    check(lib.plato_rmat_generate(C.byref(p), C.byref(h)), "plato_rmat_generate")
+    return _take_edge_list(lib, h)
+
+
+def read_csv(path) -> tuple:
+    """Edge list from CSV text -> (V, src, dst), the reference's csv_parser
+    rules (plato/graph/parsers.hpp:226-290): `path` is a file or a directory
+    of files (read in name order, ".gz" inflated); V = largest id + 1."""
+    lib = load()
+    h = C.c_void_p()
+    check(lib.plato_edge_list_read_csv(os.fsencode(str(path)), C.byref(h)), "plato_edge_list_read_csv")
+    return _take_edge_list(lib, h)
+
+
+def write_vertex_csv(directory, values, prefix: str = "", files: int = 1, gzip: bool = False) -> None:
+    """Writes `v,value` lines for every vertex into `files` CSV files
+    <directory>/<prefix><NNNN>.csv[.gz] (float32 -> %g, uint32 -> integer),
+    the result layout of the reference's examples (example/pagerank.cc:191-200)."""
+    a = np.ascontiguousarray(values)
+    if a.dtype == np.float32:
+        kind = _lib.PLATO_VALUE_F32
+    elif a.dtype == np.uint32:
+        kind = _lib.PLATO_VALUE_U32
+    else:
+        raise TypeError("write_vertex_csv: values must be float32 or uint32")
+    check(load().plato_write_vertex_csv(os.fsencode(str(directory)), prefix.encode(), _ptr(a), kind,
+                                        a.size, files, int(gzip)), "plato_write_vertex_csv")
 
 
 class Graph:

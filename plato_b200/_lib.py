@@ -12,6 +12,7 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "libplato_b200.so"
 
 PLATO_OK, PLATO_EINVAL, PLATO_ENOMEM, PLATO_ECUDA, PLATO_ETIMEDOUT, PLATO_EBUSY, PLATO_ENOTFOUND = range(7)
+PLATO_VALUE_F32, PLATO_VALUE_U32 = 0, 1  # plato_write_vertex_csv value types
 PLATO_LEVEL_UNREACHED = 0xFFFFFFFF
 PLATO_GRAPH_RELABEL = 0x1
 PLATO_PPR_PULL, PLATO_PPR_PUSHPULL = 0, 1
@@ -109,6 +110,9 @@ SIGNATURES = {
     "plato_edge_list_info": (C.c_int, [P, u32p, u64p]),
     "plato_edge_list_data": (C.c_int, [P, C.POINTER(P), C.POINTER(P)]),
     "plato_edge_list_free": (C.c_int, [P]),
+    "plato_edge_list_read_csv": (C.c_int, [C.c_char_p, C.POINTER(P)]),
+    "plato_write_vertex_csv": (C.c_int, [C.c_char_p, C.c_char_p, P, C.c_int, C.c_uint32, C.c_uint32,
+                                         C.c_int]),
 }
 
 _lib = None

@@ -78,7 +78,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         objs = list(ex.map(lambda s: _compile(s, verbose, extra), srcs))
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc()] + ARCH + ["-shared", "-o", str(tmp)] + [str(o) for o in objs] + [
-        "-Xcompiler", "-fopenmp", "-lgomp", "-lcudart"]
+        "-Xcompiler", "-fopenmp", "-lgomp", "-lcudart", "-lz"]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)

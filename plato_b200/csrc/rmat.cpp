@@ -27,6 +27,7 @@
 
 #include "plato_b200.h"
 #include "host_common.hpp"
+#include "edge_list.hpp"
 
 namespace {
 
@@ -41,12 +42,6 @@ constexpr uint64_t kPermSalt = 0xA5A5F00DC0FFEE11ULL;
 constexpr uint64_t kDropped = ~0ULL;
 
 }  // namespace
-
-struct plato_edge_list {
-  plato_vid_t vertices = 0;
-  std::vector<plato_vid_t> src;
-  std::vector<plato_vid_t> dst;
-};
 
 extern "C" int plato_rmat_generate(const plato_rmat_params* p, plato_edge_list** out) {
   using namespace plato_b200;

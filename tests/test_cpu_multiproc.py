@@ -32,7 +32,7 @@ def _worker(rank, world, port, out):
 
 def test_max_over_ranks_gloo_world2():
     port = _free_port()
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:  # no fork of a threaded process
         out = mgr.dict()
         mp.start_processes(_worker, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
         res = dict(out)
