@@ -220,6 +220,12 @@ int plato_ppr_batch(plato_graph* g, uint32_t K, const uint64_t* seed_offsets /* 
                     float* topk_vals /* host [K*topk] or NULL */,
                     uint32_t* iterations /* host [K] or NULL */);
 
+/* The column-tile width plato_ppr_batch uses for K columns when
+ * opts->k_tile == 0: autotuned on first use (a few timed iterations per
+ * candidate width), then cached per graph and power-of-two bucket of K.
+ * No reference counterpart (the reference runs one query at a time). */
+int plato_ppr_batch_k_tile(plato_graph* g, uint32_t K, uint32_t* k_tile);
+
 /* ---- continuous-batching PPR server -------------------------------------- */
 typedef struct {
   uint32_t max_slots;        /* upper bound of live queries (columns)            */

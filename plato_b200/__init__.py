@@ -268,6 +268,12 @@ class Graph:
                                           C.byref(st)), "plato_seedset_ppr")
         return out, RunStats.from_c(st)
 
+    def ppr_batch_k_tile(self, K: int) -> int:
+        """Column-tile width the autotuner picks for K columns (cached per graph)."""
+        kt = C.c_uint32()
+        _lib.check(_lib.load().plato_ppr_batch_k_tile(self.handle, K, C.byref(kt)), "plato_ppr_batch_k_tile")
+        return int(kt.value)
+
     def ppr_batch(self, seed_sets, max_iterations: int = 100, damping: float = 0.85,
                   eps: float = 1e-6, topk: int = 0, k_tile: int = 0, ranks: bool = False):
         """Batched multi-source PPR: one query per seed set (trustrank seed-set

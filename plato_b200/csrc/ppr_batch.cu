@@ -414,40 +414,61 @@ int batch_engine::topk(const std::vector<uint32_t>& cols, uint32_t k, uint32_t* 
   return PLATO_OK;
 }
 
+// Picks the column-tile width for a batch of K columns: every candidate runs
+// full iterations over a probe of min(K rounded up, 512) live columns (all
+// its tiles in one launch, as in the real batch), best of two trials of three
+// iterations; the cost is scaled to K columns.  Cached per graph and per
+// power-of-two bucket of K.
 int batch_autotune(plato_graph* g, uint32_t K, cudaStream_t st, uint32_t* kt_out) {
   uint32_t bucket = 8;
-  while (bucket < K && bucket < 128) bucket <<= 1;
+  while (bucket < K && bucket < 1024) bucket <<= 1;
   auto it = g->batch_tuned.find(bucket);
   if (it != g->batch_tuned.end()) {
     *kt_out = it->second;
     return PLATO_OK;
   }
   const uint32_t cands[] = {8, 16, 32, 64, 128};
+  const uint32_t V = g->info.vertices;
   double best = 1e300;
   uint32_t best_kt = 32;
   cudaEvent_t e0, e1;
   PLATO_CUDA_TRY(cudaEventCreate(&e0));
   PLATO_CUDA_TRY(cudaEventCreate(&e1));
+  int rc = PLATO_OK;
   for (uint32_t kt : cands) {
     if (kt > bucket) break;
+    // probe columns: up to 512, at most 8 GiB of state (two V x probe matrices)
+    const uint64_t fit = (8ull << 30) / (8ull * std::max(V, 1u));
+    const uint32_t cap = static_cast<uint32_t>(std::min<uint64_t>(512, std::max<uint64_t>(fit, kt)));
+    const uint32_t probe = std::max(kt, std::min((bucket + kt - 1) / kt * kt, cap / kt * kt));
     batch_engine eng(g);
-    PLATO_TRY(eng.init(kt, kt, 1u << 30, 0.85, 0.0, st));
-    std::vector<uint32_t> cols(kt);
-    std::vector<std::vector<uint32_t>> seeds(kt, std::vector<uint32_t>{0});
-    for (uint32_t q = 0; q < kt; ++q) cols[q] = q;
-    PLATO_TRY(eng.admit(cols, seeds));
+    rc = eng.init(probe, kt, 1u << 30, 0.85, 0.0, st);
+    if (rc != PLATO_OK) break;
+    std::vector<uint32_t> cols(probe);
+    std::vector<std::vector<uint32_t>> seeds(probe);
+    for (uint32_t q = 0; q < probe; ++q) {
+      cols[q] = q;
+      seeds[q].push_back(static_cast<uint32_t>((static_cast<uint64_t>(q) * 2654435761u) % V));
+    }
+    rc = eng.admit(cols, seeds);
+    if (rc != PLATO_OK) break;
     uint32_t live = 0;
-    PLATO_TRY(eng.step(&live, nullptr));
-    PLATO_CUDA_TRY(cudaEventRecord(e0, st));
-    const int reps = 3;
-    for (int r = 0; r < reps; ++r) PLATO_TRY(eng.step(&live, nullptr));
-    PLATO_CUDA_TRY(cudaEventRecord(e1, st));
-    PLATO_CUDA_TRY(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    PLATO_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
-    // cost of a whole K-column iteration with this tile width
-    const double tiles = static_cast<double>((K + kt - 1) / kt);
-    const double cost = ms / reps * tiles;
+    rc = eng.step(&live, nullptr);
+    if (rc != PLATO_OK) break;
+    float best_ms = 1e30f;
+    for (int trial = 0; trial < 2 && rc == PLATO_OK; ++trial) {
+      const int reps = 3;
+      if (cudaEventRecord(e0, st) != cudaSuccess) rc = set_error(PLATO_ECUDA, "autotune: event record failed");
+      for (int r = 0; r < reps && rc == PLATO_OK; ++r) rc = eng.step(&live, nullptr);
+      if (rc != PLATO_OK) break;
+      float ms = 0.f;
+      if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+          cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+        rc = set_error(PLATO_ECUDA, "autotune: event timing failed");
+      best_ms = std::min(best_ms, ms / reps);
+    }
+    if (rc != PLATO_OK) break;
+    const double cost = best_ms * (static_cast<double>(K) / probe);  // per K-column iteration
     if (cost < best) {
       best = cost;
       best_kt = kt;
@@ -455,6 +476,7 @@ int batch_autotune(plato_graph* g, uint32_t K, cudaStream_t st, uint32_t* kt_out
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (rc != PLATO_OK) return rc;
   g->batch_tuned[bucket] = best_kt;
   *kt_out = best_kt;
   return PLATO_OK;
@@ -463,6 +485,14 @@ int batch_autotune(plato_graph* g, uint32_t K, cudaStream_t st, uint32_t* kt_out
 }  // namespace plato_b200
 
 using namespace plato_b200;
+
+extern "C" int plato_ppr_batch_k_tile(plato_graph* g, uint32_t K, uint32_t* k_tile) {
+  if (!g || !k_tile) return set_error(PLATO_EINVAL, "plato_ppr_batch_k_tile: null argument");
+  if (K == 0) return set_error(PLATO_EINVAL, "plato_ppr_batch_k_tile: K must be >= 1");
+  std::lock_guard<std::mutex> lock(g->mu);
+  PLATO_CUDA_TRY(cudaSetDevice(g->device));
+  return batch_autotune(g, K, g->stream, k_tile);
+}
 
 extern "C" int plato_ppr_batch(plato_graph* g, uint32_t K, const uint64_t* seed_offsets,
                                const plato_vid_t* seeds, const plato_ppr_batch_opts* opts,

@@ -85,6 +85,19 @@ def test_batch_k_tiles_agree(g14, kt):
         assert _l1(out["ranks"][q], base["ranks"][q]) <= L1_TOL
 
 
+def test_batch_autotuned_k_tile_is_used(g14):
+    V, s, d, ref, g = g14
+    sets = zipf_seed_sets(ref.out_degrees(), 70, 16, 5)
+    kt = g.ppr_batch_k_tile(len(sets))
+    assert kt in (8, 16, 32, 64, 128)
+    assert g.ppr_batch_k_tile(len(sets)) == kt  # cached per graph and bucket
+    auto = g.ppr_batch(sets, max_iterations=200, eps=1e-6, ranks=True)
+    fixed = g.ppr_batch(sets, max_iterations=200, eps=1e-6, ranks=True, k_tile=kt)
+    assert np.array_equal(auto["ranks"].view(np.uint32), fixed["ranks"].view(np.uint32))
+    with pytest.raises(pb.PlatoError):
+        g.ppr_batch_k_tile(0)
+
+
 def test_batch_alone_equals_in_mix(g14):
     V, s, d, ref, g = g14
     sets = zipf_seed_sets(ref.out_degrees(), 40, 32, 4)
