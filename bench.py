@@ -430,13 +430,13 @@ def suite_batch(pb, plain_n=16, quick=False):
     for K in (64, 256, 1024):
         g.ppr_batch(sets[:K], 300, 0.85, 1e-6, topk=100)  # autotune + warm
         dts = []
-        for _ in range(3):  # median of three whole batches
+        for _ in range(5):  # median of five whole batches
             t0 = time.perf_counter()
             out = g.ppr_batch(sets[:K], 300, 0.85, 1e-6, topk=100)
             dts.append(time.perf_counter() - t0)
         dt = float(np.median(dts))
         res[f"K{K}"] = {"qps": K / dt, "s": dt, "speedup_vs_plain": K / dt / plain_qps,
-                        "iterations_max": int(out["iterations"].max()), "timing": "median of 3 batches",
+                        "iterations_max": int(out["iterations"].max()), "timing": "median of 5 batches",
                         "batches_s": dts, "k_tile_auto": g.ppr_batch_k_tile(K)}
         per_kt = {}
         for kt in (8, 16, 32, 64):

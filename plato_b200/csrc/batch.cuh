@@ -160,7 +160,7 @@ __device__ __forceinline__ void merge_search(const uint32_t* s_rowend, int nrows
 }
 
 template <int GL, int VEC>
-__global__ void __launch_bounds__(256, 5) k_batch_pull(batch_pass p0) {
+__global__ void __launch_bounds__(256, 4) k_batch_pull(batch_pass p0) {
   constexpr int KT = GL * VEC, NG = 256 / GL, TILE = kBatchTile, IPG = TILE / NG;
   const batch_pass p = batch_tile_view<KT>(p0);
   __shared__ uint32_t s_rowend[TILE];

@@ -26,9 +26,9 @@ class batch_engine {
            cudaStream_t st);
   // Starts columns `cols` with the given seed lists (seeds[i] for cols[i]).
   int admit(const std::vector<uint32_t>& cols, const std::vector<std::vector<uint32_t>>& seeds);
-  // One iteration over all live columns; *live = columns still running,
-  // retired = columns that finished during this iteration.
-  int step(uint32_t* live, std::vector<uint32_t>* retired);
+  // n iterations over all live columns, then one host poll; *live = columns
+  // still running, retired = columns that finished during these iterations.
+  int step(uint32_t* live, std::vector<uint32_t>* retired, uint32_t n = 1);
   // Top-k (caller ids, descending rank, ties by smaller id) of finished columns.
   int topk(const std::vector<uint32_t>& cols, uint32_t k, uint32_t* ids, float* vals);
   // Full rank vectors of finished columns, caller-id order, [cols.size()][V].

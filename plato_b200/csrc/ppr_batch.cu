@@ -12,6 +12,7 @@ namespace plato_b200 {
 namespace {
 
 constexpr int kKernelsPerIteration = 4;
+constexpr uint32_t kBatchItersPerPoll = 8;
 
 bool kt_supported(uint32_t kt) { return kt == 8 || kt == 16 || kt == 32 || kt == 64 || kt == 128; }
 // Every lane gathers a float4 (4 columns, 16 bytes) per edge; kt/4 lanes
@@ -164,7 +165,9 @@ int batch_engine::launch_iteration(int parity) {
   p.thead = thead_.p;
   p.partials = partials_.p;
   const uint32_t T = mt.count;
-  PLATO_CUDA_TRY(cudaMemsetAsync(counters_.p, 0, 2 * sizeof(uint32_t), st_));
+  // live count restarts every iteration; the retired list accumulates over
+  // the iterations of one step() and is reset there
+  PLATO_CUDA_TRY(cudaMemsetAsync(counters_.p, 0, sizeof(uint32_t), st_));
   const uint32_t fix_blocks = rows_ - T;
   switch (kt_) {
     case 8: PLATO_TRY((launch_pass<2, 4>(p, T, fix_blocks, ntiles_, st_))); break;
@@ -297,14 +300,17 @@ int batch_engine::admit(const std::vector<uint32_t>& cols,
   return rebuild_seed_index();  // synchronises before the temporaries go
 }
 
-int batch_engine::step(uint32_t* live, std::vector<uint32_t>* retired) {
-  {
-    prof_scope ps("batch_iteration", st_);
-    PLATO_CUDA_TRY(cudaGraphLaunch(exec_[cur_], st_));
+int batch_engine::step(uint32_t* live, std::vector<uint32_t>* retired, uint32_t n) {
+  PLATO_CUDA_TRY(cudaMemsetAsync(counters_.p + 1, 0, sizeof(uint32_t), st_));
+  for (uint32_t i = 0; i < std::max(n, 1u); ++i) {
+    {
+      prof_scope ps("batch_iteration", st_);
+      PLATO_CUDA_TRY(cudaGraphLaunch(exec_[cur_], st_));
+    }
+    count_launch(kKernelsPerIteration);
+    cur_ ^= 1;
   }
-  count_launch(kKernelsPerIteration);
   PLATO_CUDA_TRY(cudaStreamSynchronize(st_));
-  cur_ ^= 1;
   *live = h_counters_[0];
   const uint32_t nret = std::min(h_counters_[1], Kp_);
   if (retired) {
@@ -527,7 +533,9 @@ extern "C" int plato_ppr_batch(plato_graph* g, uint32_t K, const uint64_t* seed_
   PLATO_TRY(eng.init(K, kt, opts->max_iterations, opts->damping, opts->eps, st));
   PLATO_TRY(eng.admit(cols, sets));
   uint32_t live = K;
-  while (live > 0) PLATO_TRY(eng.step(&live, nullptr));
+  // several iterations per host poll: the device state machine idles the
+  // finished columns, and a busy host cannot stall the device between polls
+  while (live > 0) PLATO_TRY(eng.step(&live, nullptr, kBatchItersPerPoll));
   if (iterations) {
     std::vector<uint32_t> it;
     PLATO_TRY(eng.iterations(&it));
