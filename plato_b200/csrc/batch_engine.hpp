@@ -62,6 +62,20 @@ class batch_engine {
   dbuf<double> partials_;
   dbuf<uint32_t> seed_off_, seed_col_;
   dbuf<float> seed_tele_;
+  // seed-index build on the device: per-vertex counts, scan scratch and the
+  // uploaded entry list (vertex, column, rank within the vertex, teleport)
+  dbuf<uint32_t> seed_cnt_;
+  dbuf<unsigned char> scan_tmp_;
+  size_t scan_bytes_ = 0;
+  dbuf<uint32_t> ent_v_, ent_q_, ent_r_;
+  dbuf<float> ent_t_;
+  // admission / release / top-k scratch (grow-only, so no allocation per request)
+  dbuf<uint32_t> adm_cols_, adm_sv_, adm_sq_;
+  dbuf<float> adm_init_;
+  dbuf<uint32_t> tk_cols_, tk_hist_, tk_ids_, tk_undone_;
+  dbuf<unsigned char> tk_state_;  // topk_col per column
+  dbuf<unsigned long long> tk_cand_;
+  dbuf<float> tk_vals_;
   dbuf<uint32_t> counters_;  // [0] live, [1] retired count
   dbuf<uint32_t> retired_;
   uint32_t* h_counters_ = nullptr;

@@ -3,6 +3,8 @@
 #include <new>
 #include <set>
 
+#include <cub/device/device_scan.cuh>
+
 #include "batch.cuh"
 #include "batch_engine.hpp"
 #include "profile.cuh"
@@ -83,6 +85,25 @@ int upload(dbuf<T>& d, const std::vector<T>& h, cudaStream_t st) {
   return PLATO_OK;
 }
 
+// Seed index on the device: cnt[v] = number of (v, column) seed entries.
+__global__ void k_seed_count(const uint32_t* __restrict__ ev, uint32_t n, uint32_t* cnt) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    atomicAdd(&cnt[ev[i]], 1u);
+}
+
+// Entry i goes to slot off[v] + rank (entries arrive sorted by (v, column),
+// rank = position among the entries of v), so the layout is deterministic.
+__global__ void k_seed_scatter(const uint32_t* __restrict__ ev, const uint32_t* __restrict__ eq,
+                               const uint32_t* __restrict__ er, const float* __restrict__ et,
+                               uint32_t n, const uint32_t* __restrict__ off, uint32_t* col,
+                               float* tele) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t slot = off[ev[i]] + er[i];
+    col[slot] = eq[i];
+    tele[slot] = et[i];
+  }
+}
+
 }  // namespace
 
 batch_engine::~batch_engine() {
@@ -124,6 +145,12 @@ int batch_engine::init(uint32_t K, uint32_t kt, uint32_t max_iterations, double 
   PLATO_TRY(thead_.alloc(static_cast<size_t>(ntiles_) * T * kt));
   PLATO_TRY(partials_.alloc(static_cast<size_t>(ntiles_) * rows_ * kt));
   PLATO_TRY(seed_off_.alloc(static_cast<size_t>(V) + 1));
+  PLATO_TRY(seed_cnt_.alloc(static_cast<size_t>(V)));
+  if (scan_bytes_ == 0) {
+    PLATO_CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, scan_bytes_, seed_cnt_.p, seed_off_.p + 1,
+                                                 static_cast<int>(V), st_));
+    PLATO_TRY(scan_tmp_.alloc(std::max<size_t>(scan_bytes_, 1)));
+  }
   PLATO_TRY(seed_col_.alloc(static_cast<size_t>(Kp_) * 64));
   PLATO_TRY(seed_tele_.alloc(static_cast<size_t>(Kp_) * 64));
   PLATO_TRY(counters_.alloc(2));
@@ -211,6 +238,10 @@ int batch_engine::capture() {
   return PLATO_OK;
 }
 
+// Seed index (teleport entries by vertex) of every live column.  The host
+// lists the entries (a few per column), sorted by (vertex, column); the
+// device counts them per vertex, scans the counts into offsets and scatters
+// the entries, so no V-sized array crosses PCIe or is touched on the host.
 int batch_engine::rebuild_seed_index() {
   const uint32_t V = g_->info.vertices;
   struct ent {
@@ -227,27 +258,40 @@ int batch_engine::rebuild_seed_index() {
   std::sort(ents.begin(), ents.end(), [](const ent& a, const ent& b) {
     return a.v != b.v ? a.v < b.v : a.q < b.q;
   });
-  std::vector<uint32_t> off(static_cast<size_t>(V) + 1, 0), col(ents.size());
-  std::vector<float> tele(ents.size());
-  for (size_t i = 0; i < ents.size(); ++i) {
-    off[ents[i].v + 1]++;
-    col[i] = ents[i].q;
-    tele[i] = ents[i].tele;
+  const size_t n = ents.size();
+  std::vector<uint32_t> hv(n), hq(n), hr(n);
+  std::vector<float> ht(n);
+  for (size_t i = 0; i < n; ++i) {
+    hv[i] = ents[i].v;
+    hq[i] = ents[i].q;
+    ht[i] = ents[i].tele;
+    hr[i] = (i > 0 && ents[i - 1].v == ents[i].v) ? hr[i - 1] + 1 : 0;
   }
-  for (uint32_t v = 0; v < V; ++v) off[v + 1] += off[v];
   bool recapture = false;
-  if (ents.size() > seed_col_.n) {
-    PLATO_TRY(seed_col_.alloc(ents.size() * 2));
-    PLATO_TRY(seed_tele_.alloc(ents.size() * 2));
+  if (n > seed_col_.n) {
+    PLATO_TRY(seed_col_.alloc(n * 2));
+    PLATO_TRY(seed_tele_.alloc(n * 2));
     recapture = true;
   }
-  PLATO_CUDA_TRY(cudaMemcpyAsync(seed_off_.p, off.data(), off.size() * sizeof(uint32_t),
-                                 cudaMemcpyHostToDevice, st_));
-  if (!ents.empty()) {
-    PLATO_CUDA_TRY(cudaMemcpyAsync(seed_col_.p, col.data(), col.size() * sizeof(uint32_t),
-                                   cudaMemcpyHostToDevice, st_));
-    PLATO_CUDA_TRY(cudaMemcpyAsync(seed_tele_.p, tele.data(), tele.size() * sizeof(float),
-                                   cudaMemcpyHostToDevice, st_));
+  PLATO_TRY(upload(ent_v_, hv, st_));
+  PLATO_TRY(upload(ent_q_, hq, st_));
+  PLATO_TRY(upload(ent_r_, hr, st_));
+  PLATO_TRY(upload(ent_t_, ht, st_));
+  PLATO_CUDA_TRY(cudaMemsetAsync(seed_cnt_.p, 0, static_cast<size_t>(V) * sizeof(uint32_t), st_));
+  PLATO_CUDA_TRY(cudaMemsetAsync(seed_off_.p, 0, sizeof(uint32_t), st_));
+  const uint32_t n32 = static_cast<uint32_t>(n);
+  if (n32) {
+    k_seed_count<<<grid_for(n32, 256), 256, 0, st_>>>(ent_v_.p, n32, seed_cnt_.p);
+    PLATO_LAUNCHED("k_seed_count");
+  }
+  size_t tmp = scan_bytes_;
+  PLATO_CUDA_TRY(cub::DeviceScan::InclusiveSum(scan_tmp_.p, tmp, seed_cnt_.p, seed_off_.p + 1,
+                                               static_cast<int>(V), st_));
+  count_launch();
+  if (n32) {
+    k_seed_scatter<<<grid_for(n32, 256), 256, 0, st_>>>(ent_v_.p, ent_q_.p, ent_r_.p, ent_t_.p, n32,
+                                                        seed_off_.p, seed_col_.p, seed_tele_.p);
+    PLATO_LAUNCHED("k_seed_scatter");
   }
   PLATO_CUDA_TRY(cudaStreamSynchronize(st_));  // host vectors go out of scope
   if (recapture) PLATO_TRY(capture());
@@ -280,21 +324,19 @@ int batch_engine::admit(const std::vector<uint32_t>& cols,
       init.push_back(iv);
     }
   }
-  dbuf<uint32_t> d_cols, d_sv, d_sq;
-  dbuf<float> d_init;
-  PLATO_TRY(upload(d_cols, cols, st_));
-  PLATO_TRY(upload(d_sv, sv, st_));
-  PLATO_TRY(upload(d_sq, sq, st_));
-  PLATO_TRY(upload(d_init, init, st_));
+  PLATO_TRY(upload(adm_cols_, cols, st_));
+  PLATO_TRY(upload(adm_sv_, sv, st_));
+  PLATO_TRY(upload(adm_sq_, sq, st_));
+  PLATO_TRY(upload(adm_init_, init, st_));
   const uint32_t n = static_cast<uint32_t>(cols.size());
   k_zero_columns<<<grid_for(static_cast<uint64_t>(V) * n, 256), 256, 0, st_>>>(X_[cur_].p, V, kt_,
-                                                                               d_cols.p, n);
+                                                                               adm_cols_.p, n);
   PLATO_LAUNCHED("k_zero_columns");
-  k_seed_init<<<grid_for(sv.size(), 256), 256, 0, st_>>>(X_[cur_].p, V, kt_, d_sv.p, d_sq.p,
-                                                         d_init.p, static_cast<uint32_t>(sv.size()),
+  k_seed_init<<<grid_for(sv.size(), 256), 256, 0, st_>>>(X_[cur_].p, V, kt_, adm_sv_.p, adm_sq_.p,
+                                                         adm_init_.p, static_cast<uint32_t>(sv.size()),
                                                          g_->out_deg.p);
   PLATO_LAUNCHED("k_seed_init");
-  k_set_states<<<grid_for(n, 256), 256, 0, st_>>>(state_.p, iters_.p, d_cols.p, n,
+  k_set_states<<<grid_for(n, 256), 256, 0, st_>>>(state_.p, iters_.p, adm_cols_.p, n,
                                                   max_iterations_ == 1 ? COL_FINAL : COL_LIVE);
   PLATO_LAUNCHED("k_set_states");
   return rebuild_seed_index();  // synchronises before the temporaries go
@@ -323,10 +365,9 @@ int batch_engine::step(uint32_t* live, std::vector<uint32_t>* retired, uint32_t 
 
 int batch_engine::release(const std::vector<uint32_t>& cols) {
   if (cols.empty()) return PLATO_OK;
-  dbuf<uint32_t> d_cols;
-  PLATO_TRY(upload(d_cols, cols, st_));
+  PLATO_TRY(upload(adm_cols_, cols, st_));
   const uint32_t n = static_cast<uint32_t>(cols.size());
-  k_set_states<<<grid_for(n, 256), 256, 0, st_>>>(state_.p, iters_.p, d_cols.p, n, COL_FREE);
+  k_set_states<<<grid_for(n, 256), 256, 0, st_>>>(state_.p, iters_.p, adm_cols_.p, n, COL_FREE);
   PLATO_LAUNCHED("k_set_states");
   for (uint32_t q : cols) col_seeds_[q].clear();
   PLATO_CUDA_TRY(cudaStreamSynchronize(st_));
@@ -366,12 +407,14 @@ int batch_engine::topk(const std::vector<uint32_t>& cols, uint32_t k, uint32_t* 
   if (cols.empty() || k == 0) return PLATO_OK;
   if (k > kTopkMax) return set_error(PLATO_EINVAL, "topk must be <= 1024");
   const uint32_t n = static_cast<uint32_t>(cols.size());
-  dbuf<uint32_t> d_cols, hist, d_ids, undone;
-  dbuf<topk_col> st;
-  dbuf<unsigned long long> cand;
-  dbuf<float> d_vals;
+  dbuf<uint32_t>& d_cols = tk_cols_;
+  dbuf<uint32_t>& hist = tk_hist_;
+  dbuf<uint32_t>& d_ids = tk_ids_;
+  dbuf<uint32_t>& undone = tk_undone_;
+  dbuf<unsigned long long>& cand = tk_cand_;
+  dbuf<float>& d_vals = tk_vals_;
   PLATO_TRY(upload(d_cols, cols, st_));
-  PLATO_TRY(st.alloc(n));
+  PLATO_TRY(tk_state_.alloc(static_cast<size_t>(n) * sizeof(topk_col)));
   PLATO_TRY(hist.alloc(static_cast<size_t>(n) * 256));
   PLATO_TRY(cand.alloc(static_cast<size_t>(n) * kCandCap));
   PLATO_TRY(d_ids.alloc(static_cast<size_t>(n) * k));
@@ -387,7 +430,7 @@ int batch_engine::topk(const std::vector<uint32_t>& cols, uint32_t k, uint32_t* 
   j.V = g_->info.vertices;
   j.kt = kt_;
   j.to_ext = g_->relabeled ? g_->to_ext.p : nullptr;
-  j.st = st.p;
+  j.st = reinterpret_cast<topk_col*>(tk_state_.p);
   j.hist = hist.p;
   j.cand = cand.p;
   k_topk_init<<<grid_for(n, 256), 256, 0, st_>>>(j, k);
