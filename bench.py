@@ -387,6 +387,25 @@ def suite_bfs(pb, roots_n=64):
             "timing": "host clock around plato_bfs (levels not copied back)"}
 
 
+def suite_cc(pb):
+    """Connected components (label propagation on the dual-mode engine) on the
+    BFS graph: RMAT s22 ef16 seed 2 symmetrised."""
+    V, s, d = pb.rmat(22, 16, 2, symmetrize=True)
+    g = pb.Graph(V, s, d, is_directed=False)
+    g.connected_components(labels=False)
+    times = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        _, summ, st = g.connected_components(labels=False)
+        times.append(time.perf_counter() - t0)
+    g.close()
+    ms = float(np.median(times)) * 1e3
+    return {"workload": "cc_rmat_s22_ef16_seed2_sym", "vertices": V, "undirected_edges": int(s.size),
+            "ms_median": ms, "epochs": st.iterations, "push_epochs": st.push_iterations,
+            "gteps": 2 * s.size * st.iterations / (ms / 1e3) / 1e9, "summary": summ,
+            "timing": "host clock around plato_connected_components (labels not copied back), median of 5"}
+
+
 def suite_ppr_single(pb):
     """Single-source PPR on RMAT s24 seed 3 until L1 delta < 1e-7, both engines."""
     V, s, d = pb.rmat(24, 16, 3)
@@ -510,8 +529,8 @@ def run_suite(args):
     import torch  # noqa: F401  (CUDA context for the library)
     import plato_b200 as pb
     res = {"suite": True}
-    for name, fn in (("bfs", suite_bfs), ("ppr_single", suite_ppr_single), ("ppr_batch", suite_batch),
-                     ("serving", suite_serving)):
+    for name, fn in (("bfs", suite_bfs), ("cc", suite_cc), ("ppr_single", suite_ppr_single),
+                     ("ppr_batch", suite_batch), ("serving", suite_serving)):
         if args.only and name not in args.only.split(","):
             continue
         t0 = time.perf_counter()
@@ -532,7 +551,7 @@ def main():
                     help="RMAT scale (smaller values are for profiling captures only)")
     ap.add_argument("--suite", action="store_true",
                     help="also measure BFS, single PPR, batched PPR and serving (one JSON line each)")
-    ap.add_argument("--only", default="", help="with --suite: comma list of bfs,ppr_single,ppr_batch,serving")
+    ap.add_argument("--only", default="", help="with --suite: comma list of bfs,cc,ppr_single,ppr_batch,serving")
     ap.add_argument("--quick", action="store_true", help="with --suite: one small batch (profiling)")
     args = ap.parse_args()
     globals()["SCALE"] = args.scale

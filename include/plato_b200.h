@@ -171,6 +171,21 @@ int plato_seedset_ppr(plato_graph* g, const plato_vid_t* seeds, uint32_t n,
 int plato_bfs(plato_graph* g, const plato_bfs_opts* opts, const plato_dualmode_opts* engine_opts,
               uint32_t* levels, plato_vid_t* parents, plato_run_stats* stats);
 
+/* plato::algo::connected_component_t (plato/algo/cgm/connected_component.hpp):
+ * label propagation with the engine's push/pull switch (:173-245) and the
+ * component summary (:247-340).  labels: host [V] or NULL, each vertex's
+ * label = the smallest caller id that reaches it along edges (its
+ * component's smallest id on undirected graphs).  stats->iterations = epochs. */
+typedef struct {
+  uint64_t    components;      /* distinct labels                                      */
+  plato_vid_t major_label;     /* label of the largest component (ties: smallest label) */
+  uint64_t    major_vertices;
+  uint64_t    major_edges;     /* in-edges whose source has the major label; undirected: halved */
+} plato_cc_summary;
+int plato_connected_components(plato_graph* g, const plato_dualmode_opts* engine_opts,
+                               plato_vid_t* labels, plato_cc_summary* summary,
+                               plato_run_stats* stats);
+
 /* ---- algorithms (device output buffers, caller's CUDA stream) ------------- */
 /* Same as plato_pagerank but writes the ranks to device memory d_ranks [V]
  * (caller ids) on `stream` (a cudaStream_t; NULL = legacy default stream).

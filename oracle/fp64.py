@@ -99,3 +99,51 @@ def bfs_levels(vertices: int, src, dst, root: int, is_directed=True) -> np.ndarr
                 lev[v] = lev[u] + 1
                 q.append(v)
     return lev
+
+
+def cc_labels(vertices: int, src, dst, is_directed=True) -> np.ndarray:
+    """Fixed point of plato::algo::connected_component_t's label propagation
+    (plato/algo/cgm/connected_component.hpp:173-245): label[v] = the smallest
+    id u with a directed path u -> v (u = v included).  On an undirected
+    graph that is the smallest id of v's component, which is what the
+    reference's own test checks with a BFS from ascending ids
+    (plato/algo/cgm/test/test_cgm.cc:81-99, 141-149).  Computed here by
+    synchronous min-propagation over the edges until nothing changes."""
+    src = np.asarray(src, dtype=np.int64)
+    dst = np.asarray(dst, dtype=np.int64)
+    if not is_directed:
+        src, dst = np.concatenate([src, dst]), np.concatenate([dst, src])
+    lab = np.arange(vertices, dtype=np.int64)
+    while True:
+        nxt = lab.copy()
+        np.minimum.at(nxt, dst, lab[src])
+        if np.array_equal(nxt, lab):
+            return lab.astype(np.uint32)
+        lab = nxt
+
+
+def cc_components_bfs(vertices: int, src, dst) -> np.ndarray:
+    """The reference test's own labelling of an undirected graph
+    (test_cgm.cc:81-99): scan ids in ascending order, BFS from each unlabelled
+    one and give its whole component that id."""
+    src = np.asarray(src, dtype=np.int64)
+    dst = np.asarray(dst, dtype=np.int64)
+    s, d = np.concatenate([src, dst]), np.concatenate([dst, src])
+    order = np.argsort(s, kind="stable")
+    s, d = s[order], d[order]
+    off = np.zeros(vertices + 1, dtype=np.int64)
+    np.add.at(off, s + 1, 1)
+    off = np.cumsum(off)
+    label = np.full(vertices, -1, dtype=np.int64)
+    for i in range(vertices):
+        if label[i] != -1:
+            continue
+        label[i] = i
+        q = deque([i])
+        while q:
+            u = q.popleft()
+            for v in d[off[u]:off[u + 1]]:
+                if label[v] == -1:
+                    label[v] = i
+                    q.append(v)
+    return label.astype(np.uint32)

@@ -311,6 +311,20 @@ class Graph:
                                   _ptr(par) if parents else None, C.byref(s)), "plato_bfs")
         return lev, par, RunStats.from_c(s)
 
+    def connected_components(self, push_threshold: float = 0.05, labels: bool = True):
+        """Label propagation (plato/algo/cgm/connected_component.hpp) ->
+        (labels uint32 [V] or None, summary dict, stats): labels[v] = smallest
+        caller id reaching v (component minimum on undirected graphs)."""
+        lab = np.empty(self.vertices, dtype=np.uint32) if labels else None
+        eo = _lib.DualmodeOpts(push_threshold)
+        sm = _lib.CcSummary()
+        s = _lib.RunStats()
+        check(self._lib.plato_connected_components(self.handle, C.byref(eo), _ptr(lab) if labels else None,
+                                                   C.byref(sm), C.byref(s)), "plato_connected_components")
+        summary = {"components": int(sm.components), "major_label": int(sm.major_label),
+                   "major_vertices": int(sm.major_vertices), "major_edges": int(sm.major_edges)}
+        return lab, summary, RunStats.from_c(s)
+
 
 # ---- reference-shaped entry points -------------------------------------------
 

@@ -49,6 +49,11 @@ class RunStats(C.Structure):
                 ("visited", C.c_uint64), ("mode_trace", C.c_uint64)]
 
 
+class CcSummary(C.Structure):
+    _fields_ = [("components", C.c_uint64), ("major_label", C.c_uint32), ("major_vertices", C.c_uint64),
+                ("major_edges", C.c_uint64)]
+
+
 class GraphDeviceView(C.Structure):
     _fields_ = [("vertices", C.c_uint32), ("is_directed", C.c_int32), ("edges", C.c_uint64),
                 ("stored_edges", C.c_uint64), ("in_offsets", C.c_void_p), ("in_adj", C.c_void_p),
@@ -94,6 +99,8 @@ SIGNATURES = {
     "plato_graph_device_bytes": (C.c_int, [P, u64p]),
     "plato_pagerank": (C.c_int, [P, C.POINTER(PagerankOpts), P, C.POINTER(RunStats)]),
     "plato_personalized_pagerank": (C.c_int, [P, C.POINTER(PprOpts), C.c_int, P, C.POINTER(RunStats)]),
+    "plato_connected_components": (C.c_int, [P, C.POINTER(DualmodeOpts), P, C.POINTER(CcSummary),
+                                            C.POINTER(RunStats)]),
     "plato_bfs": (C.c_int, [P, C.POINTER(BfsOpts), C.POINTER(DualmodeOpts), P, P, C.POINTER(RunStats)]),
     "plato_seedset_ppr": (C.c_int, [P, P, C.c_uint32, C.POINTER(PprOpts), P, C.POINTER(RunStats)]),
     "plato_pagerank_device": (C.c_int, [P, C.POINTER(PagerankOpts), P, P, C.POINTER(RunStats)]),

@@ -128,15 +128,33 @@ __device__ __forceinline__ void bfs_pull_step(const bfs_level_args& a) {
   const uint32_t* cur = a.cur.bits;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t rounds = (a.V + stride - 1) / stride;
+  // the next row's visited bit and offsets are loaded one round ahead (only
+  // this thread can mark its own rows visited during a pull step)
+  uint64_t v_next = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  bool todo_next = false;
+  uint64_t b_next = 0, e_next = 0;
+  if (v_next < a.V && !test_bit(a.visited, static_cast<uint32_t>(v_next))) {
+    todo_next = true;
+    b_next = a.in_off[v_next];
+    e_next = a.in_off[v_next + 1];
+  }
   for (uint64_t r = 0; r < rounds; ++r) {  // warp-uniform trip count
-    const uint64_t v64 = r * stride + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t v64 = v_next;
     const uint32_t v = static_cast<uint32_t>(v64);
+    const bool todo = todo_next;
+    const uint64_t b = b_next;
+    uint64_t e = e_next;
+    v_next = v64 + stride;
+    todo_next = false;
+    if (v_next < a.V && !test_bit(a.visited, static_cast<uint32_t>(v_next))) {
+      todo_next = true;
+      b_next = a.in_off[v_next];
+      e_next = a.in_off[v_next + 1];
+    }
     bool found = false, open = false;
     uint32_t par = 0;
-    uint64_t next_edge = 0, e = 0;
-    if (v64 < a.V && !test_bit(a.visited, v)) {
-      const uint64_t b = a.in_off[v];
-      e = a.in_off[v + 1];
+    uint64_t next_edge = 0;
+    if (todo) {
       const bool p0 = b < e, p1 = b + 1 < e, p2 = b + 2 < e, p3 = b + 3 < e;
       const uint32_t s0 = p0 ? a.in_adj[b] : 0u;
       const uint32_t s1 = p1 ? a.in_adj[b + 1] : 0u;
@@ -151,10 +169,10 @@ __device__ __forceinline__ void bfs_pull_step(const bfs_level_args& a) {
       next_edge = b + 4;
       open = !found && next_edge < e;
     }
-    unsigned todo = __ballot_sync(0xffffffffu, open);
-    while (todo) {  // warp-uniform
-      const int l = __ffs(todo) - 1;
-      todo &= todo - 1;
+    unsigned open_rows = __ballot_sync(0xffffffffu, open);
+    while (open_rows) {  // warp-uniform
+      const int l = __ffs(open_rows) - 1;
+      open_rows &= open_rows - 1;
       const uint64_t rb = __shfl_sync(0xffffffffu, next_edge, l);
       const uint64_t re = __shfl_sync(0xffffffffu, e, l);
       for (uint64_t i = rb + lane; i - lane < re; i += 32) {
@@ -175,7 +193,7 @@ __device__ __forceinline__ void bfs_pull_step(const bfs_level_args& a) {
   }
 }
 
-__global__ void __launch_bounds__(256) k_bfs_level(bfs_level_args a) {
+__global__ void __launch_bounds__(256, 8) k_bfs_level(bfs_level_args a) {
   __shared__ bool s_last;
   bfs_control* c = a.ctrl;
   if (c->done) return;  // uniform: the search ended at an earlier level

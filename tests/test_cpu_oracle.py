@@ -123,3 +123,16 @@ def test_oracle_bfs_vs_serial(directed):
 
 def test_oracle_thread_count_reported():
     assert oracle.max_threads() >= 1
+
+
+def test_cc_oracle_matches_reference_test_labelling(golden):
+    """cc_labels (min-propagation fixed point) equals the reference test's
+    BFS-from-ascending-ids labelling (test_cgm.cc:81-99) on its fixture."""
+    from oracle import fp64
+    graphs, _ = golden
+    g0 = graphs["v100_e2150_ua_c3.csv"]
+    s, d = g0["src"], g0["dst"]
+    V = int(max(s.max(), d.max())) + 1
+    lab = fp64.cc_labels(V, s, d, False)
+    assert (lab == fp64.cc_components_bfs(V, s, d)).all()
+    assert (lab <= np.arange(V)).all()
