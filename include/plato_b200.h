@@ -166,6 +166,26 @@ int plato_personalized_pagerank(plato_graph* g, const plato_ppr_opts* opts, int 
  * (init 1/|S| on seeds, teleport (1-d)/|S| on seeds; opts->src is ignored). */
 int plato_seedset_ppr(plato_graph* g, const plato_vid_t* seeds, uint32_t n,
                       const plato_ppr_opts* opts, float* ranks, plato_run_stats* stats);
+
+/* Mirrors trustrank_opts_t (plato/algo/trustrank/trustrank.hpp:24-33). */
+typedef struct {
+  uint32_t iteration;      /* 100 */
+  double   damping;        /* 0.85 */
+  uint32_t seed_num;       /* 100 */
+  uint32_t select_method;  /* 0 inverse PageRank, 1 PageRank, 2 random */
+  double   eps;            /* 0.001 */
+  uint64_t random_seed;    /* method 2 only (the reference draws from std::random_device) */
+} plato_trustrank_opts;
+/* algo::trustrank with select_good_seeds (trustrank.hpp:88-259): seeds are
+ * the good vertices among the top seed_num by (inverse) PageRank (ranks of
+ * the reference's default PageRank run, FP64; ties by smaller id), or drawn
+ * at random, or every good vertex when V <= seed_num; then one seed-set PPR.
+ * good_vertices: host [V] 0/1 bytes, NULL = every vertex is good.
+ * seeds_out: host [seed_num] (sorted caller ids) or NULL; *n_seeds = count.
+ * No good seed among the selected -> PLATO_EINVAL (the reference divides
+ * by zero). */
+int plato_trustrank(plato_graph* g, const plato_trustrank_opts* opts, const uint8_t* good_vertices,
+                    float* ranks, plato_vid_t* seeds_out, uint32_t* n_seeds, plato_run_stats* stats);
 /* algo::breadth_first_search (plato/algo/bfs/bfs.hpp:55-155) with the engine's
  * push/pull switch (dualmode.hpp:245-297).  levels/parents: host [V] or NULL. */
 int plato_bfs(plato_graph* g, const plato_bfs_opts* opts, const plato_dualmode_opts* engine_opts,

@@ -154,3 +154,24 @@ class RefGraph:
         if r != 0:
             raise ValueError("ref_bfs: bad arguments")
         return lev, par, int(vis.value), int(tr.value), int(ep.value)
+
+
+def trustrank_seeds(vertices: int, src, dst, is_directed: bool, seed_num: int, select_method: int,
+                    good=None):
+    """select_good_seeds (plato/algo/trustrank/trustrank.hpp:88-146) for
+    methods 0 (inverse PageRank) and 1 (PageRank) -> (sorted seed ids, the
+    ranks used).  Ranks are the reference's default PageRank run
+    (pagerank_opts_t: 100 epochs, 0.85, eps 0.001; pagerank.hpp:39-46) on
+    the graph, transposed for method 0 (generate_rank_pairs over the
+    out-edges, trustrank.hpp:52-71); order: rank descending, id ascending."""
+    is_good = (lambda v: True) if good is None else (lambda v: bool(good[v]))
+    if vertices <= seed_num:
+        return np.array([v for v in range(vertices) if is_good(v)], dtype=np.uint32), None
+    s, d = (dst, src) if select_method == 0 else (src, dst)
+    g = RefGraph(vertices, s, d, is_directed)
+    try:
+        ranks, _, _ = g.pagerank(100, 0.85, 0.001)
+    finally:
+        g.close()
+    order = sorted(range(vertices), key=lambda v: (-ranks[v], v))[:seed_num]
+    return np.array(sorted(v for v in order if is_good(v)), dtype=np.uint32), ranks

@@ -268,6 +268,25 @@ class Graph:
                                           C.byref(st)), "plato_seedset_ppr")
         return out, RunStats.from_c(st)
 
+    def trustrank(self, good=None, iteration: int = 100, damping: float = 0.85, seed_num: int = 100,
+                  select_method: int = 0, eps: float = 0.001, random_seed: int = 0):
+        """algo::trustrank with select_good_seeds (trustrank.hpp:88-259) ->
+        (ranks float32 [V], seeds uint32 (sorted caller ids), stats).
+        good: bool/uint8 [V] or None (every vertex good); select_method 0
+        inverse PageRank, 1 PageRank, 2 random (seeded by random_seed)."""
+        V = self.vertices
+        out = np.empty(V, dtype=np.float32)
+        gv = None if good is None else np.ascontiguousarray(np.asarray(good).astype(np.uint8))
+        if gv is not None and gv.size != V:
+            raise ValueError("trustrank: good must have one entry per vertex")
+        seeds = np.empty(max(seed_num, V if V <= seed_num else 0, 1), dtype=np.uint32)
+        n = C.c_uint32()
+        o = _lib.TrustrankOpts(iteration, damping, seed_num, select_method, eps, random_seed)
+        st = _lib.RunStats()
+        check(self._lib.plato_trustrank(self.handle, C.byref(o), _ptr(gv) if gv is not None else None,
+                                        _ptr(out), _ptr(seeds), C.byref(n), C.byref(st)), "plato_trustrank")
+        return out, seeds[:n.value].copy(), RunStats.from_c(st)
+
     def ppr_batch_k_tile(self, K: int) -> int:
         """Column-tile width the autotuner picks for K columns (cached per graph)."""
         kt = C.c_uint32()

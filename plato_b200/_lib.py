@@ -49,6 +49,11 @@ class RunStats(C.Structure):
                 ("visited", C.c_uint64), ("mode_trace", C.c_uint64)]
 
 
+class TrustrankOpts(C.Structure):
+    _fields_ = [("iteration", C.c_uint32), ("damping", C.c_double), ("seed_num", C.c_uint32),
+                ("select_method", C.c_uint32), ("eps", C.c_double), ("random_seed", C.c_uint64)]
+
+
 class CcSummary(C.Structure):
     _fields_ = [("components", C.c_uint64), ("major_label", C.c_uint32), ("major_vertices", C.c_uint64),
                 ("major_edges", C.c_uint64)]
@@ -101,6 +106,8 @@ SIGNATURES = {
     "plato_personalized_pagerank": (C.c_int, [P, C.POINTER(PprOpts), C.c_int, P, C.POINTER(RunStats)]),
     "plato_connected_components": (C.c_int, [P, C.POINTER(DualmodeOpts), P, C.POINTER(CcSummary),
                                             C.POINTER(RunStats)]),
+    "plato_trustrank": (C.c_int, [P, C.POINTER(TrustrankOpts), P, P, P, C.POINTER(C.c_uint32),
+                                 C.POINTER(RunStats)]),
     "plato_bfs": (C.c_int, [P, C.POINTER(BfsOpts), C.POINTER(DualmodeOpts), P, P, C.POINTER(RunStats)]),
     "plato_seedset_ppr": (C.c_int, [P, P, C.c_uint32, C.POINTER(PprOpts), P, C.POINTER(RunStats)]),
     "plato_pagerank_device": (C.c_int, [P, C.POINTER(PagerankOpts), P, P, C.POINTER(RunStats)]),

@@ -1,0 +1,178 @@
+// TrustRank: good-seed selection, then seed-set personalized PageRank.
+//
+// Mirrors plato/algo/trustrank/trustrank.hpp:
+//   select (select_good_seeds, :88-146)
+//     V <= seed_num       every good vertex is a seed;
+//     method 0 / 1        the seed_num vertices of highest inverse PageRank
+//                         (PageRank of the transposed graph, generate_rank_pairs
+//                         over the out-edges, :52-71) or PageRank, ordered by
+//                         rank descending then id ascending, that are good;
+//     method 2            seed_num distinct vertices drawn uniformly, the good
+//                         ones kept (the reference seeds its generator from
+//                         std::random_device; here the caller's seed is used,
+//                         so a run can be repeated).
+//   trust (trustrank, :163-259)  seed-set PPR with those seeds: init 1/|S|
+//                         (divided by the out-degree) on seeds, teleport
+//                         (1-d)/|S| on seeds, eps early exit into a final
+//                         epoch -- plato_seedset_ppr on the binned pull.
+// The selection PageRank is the reference's default run (pagerank_opts_t:
+// 100 epochs, damping 0.85, eps 0.001; pagerank.hpp:39-46, 81-146) in double
+// precision, written with the reference's functor bodies for
+// include/plato_b200/dualmode.cuh (engine.reverse() for the transposed
+// graph), so the order of the ranks is the reference's up to FP64 rounding.
+#include <algorithm>
+#include <exception>
+#include <mutex>
+#include <random>
+#include <unordered_set>
+#include <vector>
+
+#include "graph.cuh"
+#include "plato_b200/dualmode.cuh"
+
+namespace plato_b200 {
+namespace {
+
+__global__ void k_tr_init(double* x, const uint32_t* __restrict__ deg, uint32_t V) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+       v += (uint64_t)gridDim.x * blockDim.x)
+    x[v] = deg[v] > 0 ? 1.0 / deg[v] : 1.0;  // pagerank.hpp:90-98
+}
+
+// pagerank.hpp:118-135: r = (1-d) + d*y; non-final epochs divide by the degree
+// and sum |x' - x| * deg into *delta.
+__global__ void k_tr_update(double* n, const double* __restrict__ c, const uint32_t* __restrict__ deg,
+                            uint32_t V, double d, int last, double* delta) {
+  double dl = 0.0;
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    double r = (1.0 - d) + d * n[v];
+    if (!last) {
+      if (deg[v] > 0) {
+        r /= deg[v];
+        dl += fabs(r - c[v]) * deg[v];
+      } else {
+        dl += fabs(r - c[v]);
+      }
+    }
+    n[v] = r;
+  }
+  dl = warp_sum(dl);
+  if ((threadIdx.x & 31) == 0 && dl != 0.0) atomicAdd(delta, dl);
+}
+
+// Ranks (caller-id order) of the reference's default PageRank on the graph
+// (transposed when `inverse`).
+std::vector<double> selection_pagerank(plato_graph* g, bool inverse) {
+  constexpr uint32_t kIterations = 100;
+  constexpr double kDamping = 0.85, kEps = 0.001;
+  dualmode_engine_t engine(g);
+  plato_graph_device_view view{};
+  if (plato_graph_get_device_view(g, &view) != PLATO_OK) throw std::runtime_error(plato_last_error());
+  if (inverse) engine.reverse();
+  // out-degrees of the structure the pull walks: in-degrees when transposed
+  const uint32_t* deg = inverse ? view.in_degree : view.out_degree;
+  const uint32_t V = engine.vertices();
+  auto curt = engine.alloc_v_state<double>();
+  auto next = engine.alloc_v_state<double>();
+  double* delta = nullptr;
+  check_cuda(cudaMalloc(&delta, sizeof(double)), "trustrank delta");
+  try {
+    k_tr_init<<<grid_for(V, 256), 256>>>(curt.data(), deg, V);
+    check_cuda(cudaGetLastError(), "k_tr_init");
+    count_launch();
+    for (uint32_t epoch = 0; epoch < kIterations; ++epoch) {
+      next.fill(0.0);
+      const double* c = curt.data();
+      double* n = next.data();
+      engine.foreach_edges<double, int>(
+          [c] __device__(const auto& context, vid_t v_i, const adj_unit_list_t& adjs) {
+            double rank_sum = 0.0;
+            for (auto it = adjs.begin_; adjs.end_ != it; ++it) rank_sum += c[it->neighbour_];
+            context.send(mepa_ag_message_t<double>{v_i, rank_sum});
+          },
+          [n] __device__(int, mepa_ag_message_t<double>& msg) -> int {
+            atomicAdd(n + msg.v_i_, msg.message_);  // write_add (atomic.hpp:97-104)
+            return 0;
+          });
+      const bool last = epoch + 1 == kIterations;
+      check_cuda(cudaMemset(delta, 0, sizeof(double)), "trustrank delta");
+      k_tr_update<<<grid_for(V, 256), 256>>>(n, c, deg, V, kDamping, last ? 1 : 0, delta);
+      check_cuda(cudaGetLastError(), "k_tr_update");
+      count_launch(3);
+      double h = 0.0;
+      check_cuda(cudaMemcpy(&h, delta, sizeof(double), cudaMemcpyDeviceToHost), "trustrank delta");
+      if (!last && h < kEps) epoch = kIterations - 2;  // pagerank.hpp:137-139
+      std::swap(curt, next);
+    }
+  } catch (...) {
+    cudaFree(delta);
+    throw;
+  }
+  cudaFree(delta);
+  return engine.to_host(curt);
+}
+
+int select_seeds(plato_graph* g, const plato_trustrank_opts* o, const uint8_t* good,
+                 std::vector<plato_vid_t>* seeds) {
+  const uint32_t V = g->info.vertices;
+  auto is_good = [good](uint32_t v) { return good == nullptr || good[v] != 0; };
+  seeds->clear();
+  if (static_cast<uint64_t>(g->info.max_v_i) + 1 <= o->seed_num) {  // trustrank.hpp:98-102
+    for (uint32_t v = 0; v < V; ++v)
+      if (is_good(v)) seeds->push_back(v);
+    return PLATO_OK;
+  }
+  if (o->select_method == 2) {  // trustrank.hpp:124-143
+    std::mt19937_64 gen(o->random_seed);
+    std::uniform_int_distribution<uint32_t> dist(0, g->info.max_v_i);
+    std::unordered_set<uint32_t> picked;
+    while (picked.size() < o->seed_num) {
+      const uint32_t v = dist(gen);
+      if (picked.insert(v).second && is_good(v)) seeds->push_back(v);
+    }
+    std::sort(seeds->begin(), seeds->end());
+    return PLATO_OK;
+  }
+  const std::vector<double> rank = selection_pagerank(g, o->select_method == 0);
+  std::vector<uint32_t> order(V);
+  for (uint32_t v = 0; v < V; ++v) order[v] = v;
+  const uint32_t k = std::min<uint32_t>(o->seed_num, V);
+  std::partial_sort(order.begin(), order.begin() + k, order.end(), [&](uint32_t a, uint32_t b) {
+    return rank[a] > rank[b] || (rank[a] == rank[b] && a < b);  // trustrank.hpp:108-112
+  });
+  for (uint32_t i = 0; i < k; ++i)
+    if (is_good(order[i])) seeds->push_back(order[i]);
+  std::sort(seeds->begin(), seeds->end());
+  return PLATO_OK;
+}
+
+}  // namespace
+}  // namespace plato_b200
+
+using namespace plato_b200;
+
+extern "C" int plato_trustrank(plato_graph* g, const plato_trustrank_opts* opts,
+                               const uint8_t* good_vertices, float* ranks, plato_vid_t* seeds_out,
+                               uint32_t* n_seeds, plato_run_stats* stats) {
+  if (!g || !opts) return set_error(PLATO_EINVAL, "plato_trustrank: null argument");
+  if (opts->select_method > 2) return set_error(PLATO_EINVAL, "plato_trustrank: select_method must be 0, 1 or 2");
+  if (opts->seed_num == 0) return set_error(PLATO_EINVAL, "plato_trustrank: seed_num must be >= 1");
+  std::vector<plato_vid_t> seeds;
+  {
+    std::lock_guard<std::mutex> lock(g->mu);
+    PLATO_CUDA_TRY(cudaSetDevice(g->device));
+    PLATO_CUDA_TRY(cudaStreamSynchronize(g->stream));  // the selection runs on the default stream
+    try {
+      PLATO_TRY(select_seeds(g, opts, good_vertices, &seeds));
+    } catch (const std::exception& e) {
+      return set_error(PLATO_ECUDA, std::string("plato_trustrank: ") + e.what());
+    }
+  }
+  if (n_seeds) *n_seeds = static_cast<uint32_t>(seeds.size());
+  if (seeds_out) std::copy(seeds.begin(), seeds.end(), seeds_out);
+  if (seeds.empty())
+    return set_error(PLATO_EINVAL, "plato_trustrank: no good vertex among the selected seeds");
+  const plato_ppr_opts po{opts->iteration, opts->damping, 0, opts->eps};
+  return plato_seedset_ppr(g, seeds.data(), static_cast<uint32_t>(seeds.size()), &po, ranks, stats);
+}
