@@ -123,7 +123,7 @@ __device__ __forceinline__ void bfs_push_step(const bfs_level_args& a) {
 // rows of a pull level stop there.  The rows still open are finished by
 // their warp, one row at a time, in rounds of 32 in-edges whose first hit is
 // found with a ballot, so the parent equals that of a one-by-one scan.
-__device__ __forceinline__ void bfs_pull_step(const bfs_level_args& a) {
+__device__ __forceinline__ void bfs_pull_step(const bfs_level_args& a, append_smem& app) {
   const unsigned lane = threadIdx.x & 31;
   const uint32_t* cur = a.cur.bits;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -189,12 +189,13 @@ __device__ __forceinline__ void bfs_pull_step(const bfs_level_args& a) {
       }
     }
     if (found) bfs_visit(a, v, par);
-    frontier_append_warp(a.next, found, v, a.out_deg);
+    frontier_append_block(a.next, found, v, a.out_deg, app);  // block-uniform: same rounds everywhere
   }
 }
 
 __global__ void __launch_bounds__(256, 8) k_bfs_level(bfs_level_args a) {
   __shared__ bool s_last;
+  __shared__ append_smem s_app;
   bfs_control* c = a.ctrl;
   if (c->done) return;  // uniform: the search ended at an earlier level
   const int mode = c->mode;
@@ -207,7 +208,7 @@ __global__ void __launch_bounds__(256, 8) k_bfs_level(bfs_level_args a) {
   if (mode == 1)
     bfs_push_step(a);
   else
-    bfs_pull_step(a);
+    bfs_pull_step(a, s_app);
 
   // the last CTA to finish sees every append (fence + ticket) and decides
   // the next level (dualmode.hpp:264-279; bfs.hpp:92 ends on no activation)

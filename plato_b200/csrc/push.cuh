@@ -77,6 +77,57 @@ __device__ __forceinline__ void frontier_append_warp(frontier_view f, bool take,
   if (lane == leader && dsum) atomicAdd(&f.counters[2], dsum);
 }
 
+// Block-collective append (every thread of the block calls, the same number
+// of times): warps reserve their slots with shared-memory atomics and one
+// thread per block takes the block's ranges from the global counters, so the
+// counters see one atomic per block and call instead of one per warp.
+struct append_smem {
+  unsigned long long base_q, base_c, dsum;
+  uint32_t cnt_q, cnt_c;
+};
+
+__device__ __forceinline__ void frontier_append_block(frontier_view f, bool take, uint32_t v,
+                                                      const uint32_t* __restrict__ deg,
+                                                      append_smem& sm) {
+  const unsigned lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    sm.cnt_q = 0;
+    sm.cnt_c = 0;
+    sm.dsum = 0;
+  }
+  __syncthreads();
+  const unsigned m = __ballot_sync(0xffffffffu, take);
+  const uint32_t dg = take ? deg[v] : 0u;
+  const uint32_t nch = (dg + kPushChunk - 1) / kPushChunk;
+  uint32_t inc = nch;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= static_cast<unsigned>(o)) inc += t;
+  }
+  const uint32_t tot = __shfl_sync(0xffffffffu, inc, 31);
+  const unsigned long long dsum = warp_sum(static_cast<unsigned long long>(dg));
+  uint32_t wq = 0, wc = 0;
+  if (lane == 0 && m) {
+    wq = atomicAdd(&sm.cnt_q, static_cast<uint32_t>(__popc(m)));
+    if (tot) wc = atomicAdd(&sm.cnt_c, tot);
+    if (dsum) atomicAdd(&sm.dsum, dsum);
+  }
+  wq = __shfl_sync(0xffffffffu, wq, 0);
+  wc = __shfl_sync(0xffffffffu, wc, 0);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (sm.cnt_q) sm.base_q = atomicAdd(&f.counters[0], static_cast<unsigned long long>(sm.cnt_q));
+    if (sm.cnt_c) sm.base_c = atomicAdd(&f.counters[1], static_cast<unsigned long long>(sm.cnt_c));
+    if (sm.dsum) atomicAdd(&f.counters[2], sm.dsum);
+  }
+  __syncthreads();
+  if (take) {
+    f.queue[sm.base_q + wq + __popc(m & ((1u << lane) - 1u))] = v;
+    for (uint32_t k = 0; k < nch; ++k) f.chunks[sm.base_c + wc + (inc - nch) + k] = make_uint2(v, k);
+  }
+}
+
 static __global__ void k_frontier_seed(frontier_view f, uint32_t v, const uint32_t* __restrict__ deg) {
   // one warp
   const bool take = (threadIdx.x == 0);
