@@ -186,24 +186,43 @@ static __global__ void k_popc(const uint32_t* w, size_t nw, unsigned long long* 
   atomicAdd(out, c);
 }
 
-// Frontier compaction + active-edge count (dualmode.hpp:264-277).
-static __global__ void k_compact(const uint32_t* bits, uint32_t n, const uint32_t* deg,
-                                 vid_t* queue, unsigned long long* counters) {
+// Frontier compaction + active-edge count (dualmode.hpp:264-277).  Warps
+// reserve queue slots in shared memory and one thread per block and round
+// takes the block's range from the global counter, so a dense frontier does
+// not serialise on one address.
+static __global__ void __launch_bounds__(256) k_compact(const uint32_t* bits, uint32_t n,
+                                                        const uint32_t* deg, vid_t* queue,
+                                                        unsigned long long* counters) {
+  __shared__ unsigned long long s_base, s_deg;
+  __shared__ uint32_t s_cnt;
   const unsigned lane = threadIdx.x & 31;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t rounds = (n + stride - 1) / stride;
-  for (uint64_t r = 0; r < rounds; ++r) {
+  for (uint64_t r = 0; r < rounds; ++r) {  // block-uniform trip count
     const uint64_t v = r * stride + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     const bool on = v < n && ((bits[v >> 5] >> (v & 31)) & 1u);
+    if (threadIdx.x == 0) {
+      s_cnt = 0;
+      s_deg = 0;
+    }
+    __syncthreads();
     const unsigned m = __ballot_sync(0xffffffffu, on);
-    unsigned long long base = 0;
-    if (lane == 0 && m) base = atomicAdd(&counters[0], static_cast<unsigned long long>(__popc(m)));
-    base = __shfl_sync(0xffffffffu, base, 0);
     unsigned long long de = on ? deg[v] : 0ull;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) de += __shfl_xor_sync(0xffffffffu, de, o);
-    if (lane == 0 && de) atomicAdd(&counters[1], de);
-    if (on) queue[base + __popc(m & ((1u << lane) - 1u))] = static_cast<vid_t>(v);
+    uint32_t wbase = 0;
+    if (lane == 0 && m) {
+      wbase = atomicAdd(&s_cnt, static_cast<uint32_t>(__popc(m)));
+      if (de) atomicAdd(&s_deg, de);
+    }
+    wbase = __shfl_sync(0xffffffffu, wbase, 0);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      if (s_cnt) s_base = atomicAdd(&counters[0], static_cast<unsigned long long>(s_cnt));
+      if (s_deg) atomicAdd(&counters[1], s_deg);
+    }
+    __syncthreads();
+    if (on) queue[s_base + wbase + __popc(m & ((1u << lane) - 1u))] = static_cast<vid_t>(v);
   }
 }
 
