@@ -87,32 +87,108 @@ __device__ __forceinline__ void bfs_visit(const bfs_level_args& a, uint32_t v, u
   atomicOr(&a.next.bits[v >> 5], bit);
 }
 
-// Push step: frontier chunks -> claim unvisited out-neighbours.
+// Claims dst for parent u if nobody has (bfs.hpp:97-118: CAS on the parent);
+// `word` is a recent read of dst's visited word (bits are only ever set, and
+// the atomic decides).
+__device__ __forceinline__ bool bfs_claim(const bfs_level_args& a, uint32_t u, uint32_t dst,
+                                          uint32_t word) {
+  const uint32_t bit = 1u << (dst & 31);
+  if (word & bit) return false;
+  if (atomicOr(&a.visited[dst >> 5], bit) & bit) return false;
+  a.level[dst] = a.new_level;
+  a.parent[dst] = u;
+  atomicOr(&a.next.bits[dst >> 5], bit);
+  return true;
+}
+
+constexpr uint32_t kPushLaneEdges = 8;  // chunks this short are walked by one lane
+
+// Push step: frontier chunks -> claim unvisited out-neighbours.  With few
+// chunks (at most four per warp) each warp walks one chunk, 32 edges a round.
+// With many, a warp takes 32 chunks at a time, one per lane, interleaved over
+// the chunk list (lane l of task t takes chunk l * tasks + t, so the chunks of
+// one hub land on different warps); a lane walks a chunk of at most
+// kPushLaneEdges edges itself (ids, then visited words, four at a time in
+// flight), and the warp walks the longer chunks together.  Large push
+// frontiers are mostly low-degree vertices with one short chunk each.
 __device__ __forceinline__ void bfs_push_step(const bfs_level_args& a) {
   const unsigned long long nchunks = a.cur.counters[1];
   const unsigned lane = threadIdx.x & 31;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t c = warp; c < nchunks; c += nwarps) {
-    const uint2 ch = a.cur.chunks[c];
-    const uint32_t u = ch.x;
-    const uint64_t b = a.out_off[u] + static_cast<uint64_t>(ch.y) * kPushChunk;
-    const uint64_t e_end = min(b + kPushChunk, a.out_off[u + 1]);
-    for (uint64_t base = b; base < e_end; base += 32) {
-      const uint64_t e = base + lane;
-      uint32_t dst = 0;
-      bool fresh = false;
-      if (e < e_end) {
-        dst = a.out_adj[e];
-        const uint32_t bit = 1u << (dst & 31);
-        if (!(a.visited[dst >> 5] & bit)) fresh = !(atomicOr(&a.visited[dst >> 5], bit) & bit);
-        if (fresh) {
-          a.level[dst] = a.new_level;
-          a.parent[dst] = u;
-          atomicOr(&a.next.bits[dst >> 5], bit);
+  if (nchunks <= 4 * nwarps) {
+    // few chunks (the first levels: hubs' long chunks): one chunk per warp,
+    // so every chunk gets its own warp
+    for (uint64_t c = warp; c < nchunks; c += nwarps) {
+      const uint2 ch = a.cur.chunks[c];
+      const uint64_t b = a.out_off[ch.x] + static_cast<uint64_t>(ch.y) * kPushChunk;
+      const uint64_t e_end = min(b + kPushChunk, a.out_off[ch.x + 1]);
+      for (uint64_t base = b; base < e_end; base += 32) {
+        const uint64_t e = base + lane;
+        uint32_t dst = 0;
+        bool fresh = false;
+        if (e < e_end) {
+          dst = a.out_adj[e];
+          fresh = bfs_claim(a, ch.x, dst, a.visited[dst >> 5]);
         }
+        frontier_append_warp(a.next, fresh, dst, a.out_deg);
       }
-      frontier_append_warp(a.next, fresh, dst, a.out_deg);
+    }
+    return;
+  }
+  const uint64_t ntasks = (nchunks + 31) / 32;
+  for (uint64_t t = warp; t < ntasks; t += nwarps) {  // warp-uniform
+    const uint64_t c = static_cast<uint64_t>(lane) * ntasks + t;
+    uint32_t u = 0;
+    uint64_t b = 0, e_end = 0;
+    if (c < nchunks) {
+      const uint2 ch = a.cur.chunks[c];
+      u = ch.x;
+      b = a.out_off[u] + static_cast<uint64_t>(ch.y) * kPushChunk;
+      e_end = min(b + kPushChunk, a.out_off[u + 1]);
+    }
+    const bool own = e_end - b <= kPushLaneEdges;  // lanes without a chunk too
+    for (uint32_t s = 0; s < kPushLaneEdges; s += 4) {
+      uint32_t d0 = 0, d1 = 0, d2 = 0, d3 = 0;
+      bool f0 = false, f1 = false, f2 = false, f3 = false;
+      if (own) {
+        const uint64_t e = b + s;
+        d0 = e < e_end ? a.out_adj[e] : 0u;
+        d1 = e + 1 < e_end ? a.out_adj[e + 1] : 0u;
+        d2 = e + 2 < e_end ? a.out_adj[e + 2] : 0u;
+        d3 = e + 3 < e_end ? a.out_adj[e + 3] : 0u;
+        // the four visited words in flight before the (rare) claims
+        const uint32_t w0 = e < e_end ? a.visited[d0 >> 5] : ~0u;
+        const uint32_t w1 = e + 1 < e_end ? a.visited[d1 >> 5] : ~0u;
+        const uint32_t w2 = e + 2 < e_end ? a.visited[d2 >> 5] : ~0u;
+        const uint32_t w3 = e + 3 < e_end ? a.visited[d3 >> 5] : ~0u;
+        f0 = e < e_end && bfs_claim(a, u, d0, w0);
+        f1 = e + 1 < e_end && bfs_claim(a, u, d1, w1);
+        f2 = e + 2 < e_end && bfs_claim(a, u, d2, w2);
+        f3 = e + 3 < e_end && bfs_claim(a, u, d3, w3);
+      }
+      frontier_append_warp(a.next, f0, d0, a.out_deg);
+      frontier_append_warp(a.next, f1, d1, a.out_deg);
+      frontier_append_warp(a.next, f2, d2, a.out_deg);
+      frontier_append_warp(a.next, f3, d3, a.out_deg);
+    }
+    unsigned big = __ballot_sync(0xffffffffu, !own);
+    while (big) {  // warp-uniform
+      const int l = __ffs(big) - 1;
+      big &= big - 1;
+      const uint32_t uu = __shfl_sync(0xffffffffu, u, l);
+      const uint64_t bb = __shfl_sync(0xffffffffu, b, l);
+      const uint64_t ee = __shfl_sync(0xffffffffu, e_end, l);
+      for (uint64_t base = bb; base < ee; base += 32) {
+        const uint64_t e = base + lane;
+        uint32_t dst = 0;
+        bool fresh = false;
+        if (e < ee) {
+          dst = a.out_adj[e];
+          fresh = bfs_claim(a, uu, dst, a.visited[dst >> 5]);
+        }
+        frontier_append_warp(a.next, fresh, dst, a.out_deg);
+      }
     }
   }
 }
