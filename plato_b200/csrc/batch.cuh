@@ -27,7 +27,7 @@ namespace plato_b200 {
 
 enum : uint8_t { COL_FREE = 0, COL_LIVE = 1, COL_FINAL = 2, COL_DONE = 3 };
 
-constexpr int kBatchTile = 1024;  // merge items per CTA: short per-group chains, many CTAs in flight
+constexpr int kBatchTile = 2048;  // merge items per CTA (1024: 5-9% slower at RMAT s22-s24)
 
 struct seed_index_view {
   const uint32_t* off;   // [V+1] by internal vertex
@@ -210,9 +210,11 @@ __global__ void __launch_bounds__(256, 4) k_batch_pull(batch_pass p0) {
     const int e_end = (r < rb) ? static_cast<int>(s_rowend[r]) : jb;
     // rounds of eight row gathers in flight per lane; the last round of a
     // row is predicated instead of a serial tail, so a row costs one gather
-    // latency per eight in-edges
+    // latency per eight in-edges.  A lane whose columns are all finished or
+    // free loads nothing (its part of the row is never fetched), so a tile
+    // costs less as its columns converge.
     for (; jj < e_end; jj += 8) {
-      const int n = e_end - jj;
+      const int n = mine ? e_end - jj : 0;
       float a[8][VEC];
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
