@@ -406,6 +406,68 @@ def suite_cc(pb):
             "timing": "host clock around plato_connected_components (labels not copied back), median of 5"}
 
 
+def _profiled(pb, names, fn):
+    """Runs fn() with the library's kernel timing on; returns {name: (ms, launches)}."""
+    import ctypes as C
+    lib = pb.load()
+    lib.plato_profile_reset()
+    lib.plato_profile_enable(1)
+    fn()
+    lib.plato_profile_enable(0)
+    out = {}
+    for name in names:
+        tot, cnt = C.c_double(), C.c_uint64()
+        lib.plato_profile_read(name.encode(), C.byref(tot), C.byref(cnt))
+        out[name] = (tot.value, int(cnt.value))
+    return out
+
+
+HLL_KERNELS = ("k_hll_rows", "k_hll_hubs", "k_hll_spread")
+
+
+def suite_hll(pb, bits=6):
+    """HyperANF and n-step degrees (HyperLogLog propagation) on the BFS graph,
+    RMAT s22 ef16 seed 2 symmetrised, P = 6 (the CLIs' default width).
+
+    Roofline of one full epoch (every row active, iteration = 1): algorithmic
+    bytes = E*m (a source row per stored edge) + 4E (ids) + 2*V*m (own row
+    read, new row written) + 16V (offsets), over the gather kernels' device
+    time; E = stored directed edges, m = 2^P."""
+    V, s, d = pb.rmat(22, 16, 2, symmetrize=True)
+    g = pb.Graph(V, s, d, is_directed=False)
+    E = 2 * int(s.size)
+    m = 1 << bits
+    out = {"workload": "hll_rmat_s22_ef16_seed2_sym", "vertices": V, "stored_edges": E, "bits": bits}
+    g.hyperanf(1, bits)
+    kt = _profiled(pb, HLL_KERNELS, lambda: g.hyperanf(1, bits))
+    dev_ms = kt["k_hll_rows"][0] + kt["k_hll_hubs"][0]
+    alg = E * m + 4 * E + 2 * V * m + 16 * V
+    peak, peak_kind = measured_peak()
+    out["full_epoch"] = {"kernel_ms": dev_ms, "rows_ms": kt["k_hll_rows"][0], "hubs_ms": kt["k_hll_hubs"][0],
+                         "algorithmic_bytes": alg, "achieved_gbs": alg / (dev_ms / 1e3) / 1e9,
+                         "frac": alg / (dev_ms / 1e3) / 1e9 / peak, "peak_source": f"{peak_kind} hbm_gbs"}
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        avg, anfs, _, st = g.hyperanf(20, bits)
+        times.append(time.perf_counter() - t0)
+    kt = _profiled(pb, HLL_KERNELS, lambda: g.hyperanf(20, bits))
+    out["hyperanf"] = {"ms_median": float(np.median(times)) * 1e3, "epochs": st.iterations,
+                       "push_epochs": st.push_iterations, "avg_distance": avg, "anfs": len(anfs),
+                       "gather_kernel_ms": kt["k_hll_rows"][0] + kt["k_hll_hubs"][0],
+                       "timing": "host clock around plato_hyperanf (iteration 20), median of 3"}
+    rng = np.random.default_rng(2)
+    for label, tg in (("all_targets", None),
+                      ("64_targets", np.isin(np.arange(V), rng.choice(V, 64, replace=False)))):
+        g.nstep_degrees(step=2, bits=bits, targets=tg)
+        t0 = time.perf_counter()
+        _, _, st = g.nstep_degrees(step=2, bits=bits, targets=tg)
+        out[f"nstep_{label}"] = {"ms": (time.perf_counter() - t0) * 1e3, "step": 2, "epochs": st.iterations,
+                                 "push_epochs": st.push_iterations}
+    g.close()
+    return out
+
+
 def suite_ppr_single(pb):
     """Single-source PPR on RMAT s24 seed 3 until L1 delta < 1e-7, both engines."""
     V, s, d = pb.rmat(24, 16, 3)
@@ -529,7 +591,7 @@ def run_suite(args):
     import torch  # noqa: F401  (CUDA context for the library)
     import plato_b200 as pb
     res = {"suite": True}
-    for name, fn in (("bfs", suite_bfs), ("cc", suite_cc), ("ppr_single", suite_ppr_single),
+    for name, fn in (("bfs", suite_bfs), ("cc", suite_cc), ("hll", suite_hll), ("ppr_single", suite_ppr_single),
                      ("ppr_batch", suite_batch), ("serving", suite_serving)):
         if args.only and name not in args.only.split(","):
             continue
@@ -551,7 +613,7 @@ def main():
                     help="RMAT scale (smaller values are for profiling captures only)")
     ap.add_argument("--suite", action="store_true",
                     help="also measure BFS, single PPR, batched PPR and serving (one JSON line each)")
-    ap.add_argument("--only", default="", help="with --suite: comma list of bfs,cc,ppr_single,ppr_batch,serving")
+    ap.add_argument("--only", default="", help="with --suite: comma list of bfs,cc,hll,ppr_single,ppr_batch,serving")
     ap.add_argument("--quick", action="store_true", help="with --suite: one small batch (profiling)")
     args = ap.parse_args()
     globals()["SCALE"] = args.scale

@@ -206,6 +206,44 @@ int plato_connected_components(plato_graph* g, const plato_dualmode_opts* engine
                                plato_vid_t* labels, plato_cc_summary* summary,
                                plato_run_stats* stats);
 
+/* ---- HyperLogLog propagation (hyperloglog_t<P>, plato/util/hyperloglog.hpp:32-142;
+ * ids hashed with murmurhash3, plato/util/hash.hpp:33-88) -------------------- */
+/* Mirrors hyperanf_opts_t (plato/algo/hyperanf/hyperanf.hpp:43-46). */
+typedef struct {
+  uint32_t iteration; /* 20 */
+  uint32_t bits;      /* register-count exponent P in [4, 16] (the CLI's --bits, default 6) */
+} plato_hyperanf_opts;
+/* algo::hyperanf (hyperanf.hpp:83-195): *avg_distance = GetAvgDistance of the
+ * ANF series (NaN when the series never grows).  anfs: host [iteration + 1] or
+ * NULL, *n_anfs = entries written.  registers: host [V << bits] or NULL, the
+ * final register rows in caller-id order.  stats: epochs and the engine's
+ * push/pull choice per epoch. */
+int plato_hyperanf(plato_graph* g, const plato_hyperanf_opts* opts, const plato_dualmode_opts* engine_opts,
+                   double* avg_distance, double* anfs, uint32_t* n_anfs, uint8_t* registers,
+                   plato_run_stats* stats);
+
+#define PLATO_NSTEP_IN 1
+#define PLATO_NSTEP_OUT 2
+#define PLATO_NSTEP_BOTH 3
+/* Mirrors nstepdegree_opts_t (plato/algo/nstepdegrees/nstepdegrees.hpp:47-51)
+ * plus the register width the reference takes as a template argument. */
+typedef struct {
+  uint32_t step;        /* epochs per phase; 0xFFFFFFFF = until nothing changes (the CLI's -1) */
+  uint32_t bits;        /* P in [4, 16] (CLI default 6) */
+  uint32_t type;        /* PLATO_NSTEP_IN / _OUT / _BOTH ("in" / "out" / "both") */
+  int32_t  is_directed; /* nstepdegree_opts_t::is_directed: with type BOTH and 0, out = in */
+} plato_nstep_opts;
+/* nstepdegrees_t::compute (nstepdegrees.hpp:380-402): for each target, the
+ * estimated number of vertices within `step` hops towards it (in) or from it
+ * (out), excluding itself.  targets: host [V] 0/1 bytes by caller id, NULL =
+ * every vertex (the CLI's "ALL").  in_degrees / out_degrees: host [V] or NULL,
+ * caller ids, 0 for non-targets.  The engine's switch and the reference's
+ * forward push in reversed phases are reproduced (see nstepdegrees.hpp:217-229,
+ * 316-327). */
+int plato_nstep_degrees(plato_graph* g, const plato_nstep_opts* opts, const plato_dualmode_opts* engine_opts,
+                        const uint8_t* targets, plato_vid_t* in_degrees, plato_vid_t* out_degrees,
+                        plato_run_stats* stats);
+
 /* ---- algorithms (device output buffers, caller's CUDA stream) ------------- */
 /* Same as plato_pagerank but writes the ranks to device memory d_ranks [V]
  * (caller ids) on `stream` (a cudaStream_t; NULL = legacy default stream).

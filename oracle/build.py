@@ -25,5 +25,29 @@ def build(force: bool = False) -> Path:
     return LIB
 
 
+REF_ROOT = Path("/root/reference")
+REF_SHIM = HERE / "hll_ref_shim.cpp"
+REF_LIB = HERE / "_ref" / "libhll_ref.so"
+
+
+def build_ref(force: bool = False, ref_root: Path = REF_ROOT) -> Path | None:
+    """Compile oracle/_ref/libhll_ref.so: hll_ref_shim.cpp over the reference's
+    own plato/util/hyperloglog.hpp + hash.hpp, read where they lie in the
+    reference tree (header-only, no dependencies).  Returns None when the
+    reference tree is absent (the committed golden vectors stand in)."""
+    if not (ref_root / "plato" / "util" / "hyperloglog.hpp").exists():
+        return None
+    if not force and REF_LIB.exists() and REF_LIB.stat().st_mtime >= REF_SHIM.stat().st_mtime:
+        return REF_LIB
+    REF_LIB.parent.mkdir(exist_ok=True)
+    tmp = REF_LIB.with_suffix(".so.tmp")
+    cmd = ["g++", "-O2", "-fPIC", "-shared", "-std=c++14", "-I", str(ref_root), "-o", str(tmp),
+           str(REF_SHIM)]
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, REF_LIB)
+    return REF_LIB
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv))
+    print(build_ref(force="--force" in sys.argv))

@@ -344,6 +344,49 @@ class Graph:
                    "major_vertices": int(sm.major_vertices), "major_edges": int(sm.major_edges)}
         return lab, summary, RunStats.from_c(s)
 
+    def hyperanf(self, iteration: int = 20, bits: int = 6, push_threshold: float = 0.05,
+                 registers: bool = False):
+        """algo::hyperanf (plato/algo/hyperanf/hyperanf.hpp:83-195) ->
+        (avg_distance, anfs float64 [n], registers uint8 [V, 2^bits] or None,
+        stats)."""
+        o = _lib.HyperanfOpts(iteration, bits)
+        eo = _lib.DualmodeOpts(push_threshold)
+        avg = C.c_double()
+        anfs = np.empty(iteration + 1, dtype=np.float64)
+        n = C.c_uint32()
+        regs = np.empty((self.vertices, 1 << bits), dtype=np.uint8) if registers and 4 <= bits <= 16 else None
+        s = _lib.RunStats()
+        check(self._lib.plato_hyperanf(self.handle, C.byref(o), C.byref(eo), C.byref(avg), _ptr(anfs),
+                                       C.byref(n), _ptr(regs) if regs is not None else None, C.byref(s)),
+              "plato_hyperanf")
+        return float(avg.value), anfs[: n.value].copy(), regs, RunStats.from_c(s)
+
+    def nstep_degrees(self, step: int = 20, bits: int = 6, kind: str = "both", is_directed=None,
+                      targets=None, push_threshold: float = 0.05):
+        """nstepdegrees_t::compute (plato/algo/nstepdegrees/nstepdegrees.hpp:380-402)
+        -> (in_degrees uint32 [V], out_degrees uint32 [V], stats); step < 0
+        means until nothing changes (the CLI's -1); targets: bool [V] by
+        caller id or None for every vertex."""
+        kinds = {"in": 1, "out": 2, "both": 3}
+        if kind not in kinds:
+            raise PlatoError(1, "nstep_degrees", f"kind must be in/out/both, got {kind!r}")
+        if is_directed is None:
+            is_directed = self.info.is_directed_
+        o = _lib.NstepOpts(0xFFFFFFFF if step < 0 else step, bits, kinds[kind], int(bool(is_directed)))
+        eo = _lib.DualmodeOpts(push_threshold)
+        tg = None
+        if targets is not None:
+            tg = np.ascontiguousarray(np.asarray(targets, dtype=bool).astype(np.uint8))
+            if tg.size != self.vertices:
+                raise PlatoError(1, "nstep_degrees", "targets must have one entry per vertex")
+        din = np.empty(self.vertices, dtype=np.uint32)
+        dout = np.empty(self.vertices, dtype=np.uint32)
+        s = _lib.RunStats()
+        check(self._lib.plato_nstep_degrees(self.handle, C.byref(o), C.byref(eo),
+                                            _ptr(tg) if tg is not None else None, _ptr(din), _ptr(dout),
+                                            C.byref(s)), "plato_nstep_degrees")
+        return din, dout, RunStats.from_c(s)
+
 
 # ---- reference-shaped entry points -------------------------------------------
 

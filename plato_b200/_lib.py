@@ -59,6 +59,14 @@ class CcSummary(C.Structure):
                 ("major_edges", C.c_uint64)]
 
 
+class HyperanfOpts(C.Structure):
+    _fields_ = [("iteration", C.c_uint32), ("bits", C.c_uint32)]
+
+
+class NstepOpts(C.Structure):
+    _fields_ = [("step", C.c_uint32), ("bits", C.c_uint32), ("type", C.c_uint32), ("is_directed", C.c_int32)]
+
+
 class GraphDeviceView(C.Structure):
     _fields_ = [("vertices", C.c_uint32), ("is_directed", C.c_int32), ("edges", C.c_uint64),
                 ("stored_edges", C.c_uint64), ("in_offsets", C.c_void_p), ("in_adj", C.c_void_p),
@@ -108,6 +116,10 @@ SIGNATURES = {
                                             C.POINTER(RunStats)]),
     "plato_trustrank": (C.c_int, [P, C.POINTER(TrustrankOpts), P, P, P, C.POINTER(C.c_uint32),
                                  C.POINTER(RunStats)]),
+    "plato_hyperanf": (C.c_int, [P, C.POINTER(HyperanfOpts), C.POINTER(DualmodeOpts), C.POINTER(C.c_double),
+                                P, C.POINTER(C.c_uint32), P, C.POINTER(RunStats)]),
+    "plato_nstep_degrees": (C.c_int, [P, C.POINTER(NstepOpts), C.POINTER(DualmodeOpts), P, P, P,
+                                     C.POINTER(RunStats)]),
     "plato_bfs": (C.c_int, [P, C.POINTER(BfsOpts), C.POINTER(DualmodeOpts), P, P, C.POINTER(RunStats)]),
     "plato_seedset_ppr": (C.c_int, [P, P, C.c_uint32, C.POINTER(PprOpts), P, C.POINTER(RunStats)]),
     "plato_pagerank_device": (C.c_int, [P, C.POINTER(PagerankOpts), P, P, C.POINTER(RunStats)]),

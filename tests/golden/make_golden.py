@@ -6,9 +6,13 @@ Reads the reference's fixture graphs (data/graph/*.csv) with the reference's
 CSV rules (plato/graph/parsers.hpp:226-290: `src,dst[,w]` per line, fields
 split on ',', parsed with strtoul so surrounding blanks are tolerated, empty
 lines skipped) and writes
-  fixtures.npz  edge lists (uint32) of the fixture graphs,
-  kats.json     the known-answer values the reference's own substrate tests
-                assert on those graphs, each with its file:line.
+  fixtures.npz    edge lists (uint32) of the fixture graphs,
+  kats.json       the known-answer values the reference's own tests assert on
+                  those graphs, each with its file:line,
+  hll_golden.npz  murmurhash3 values, HyperLogLog registers and estimates
+                  computed by the reference's own plato/util/hash.hpp and
+                  plato/util/hyperloglog.hpp (compiled from the reference tree
+                  by oracle/build.py build_ref into oracle/_ref/).
 The reference tree is only needed to regenerate; tests read the outputs.
 """
 from __future__ import annotations
@@ -20,7 +24,7 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-GRAPHS = ["graph_10_9.csv", "v100_e2150_ua_c3.csv", "v100_e4300_da_c3.csv"]
+GRAPHS = ["graph_10_9.csv", "v100_e2150_ua_c3.csv", "v100_e4300_da_c3.csv", "raw_graph_7_7.csv"]
 
 
 def parse_csv(path: Path) -> tuple[np.ndarray, np.ndarray]:
@@ -66,7 +70,60 @@ KATS = {
          "values": [0, 1, 1, 1, 1, 1, 1, 1, 1, 1],
          "source": "plato/graph/test/message_passing.cc:62-87"},
     ],
+    # (in, out) per vertex, directed, step 1, bits 6, type both, every vertex a target
+    "nstep_degrees": [
+        {"graph": "raw_graph_7_7.csv", "is_directed": True, "step": 1, "bits": 6, "type": "both",
+         "values": {"0": [3, 1], "4": [1, 1]},
+         "source": "plato/algo/nstepdegrees/test/test_nstepdegrees.cc:41-48,87-96,104-139"},
+    ],
+    # |hyperanf average distance - exact average distance| <= tolerance
+    "hyperanf": [
+        {"graph": "raw_graph_7_7.csv", "is_directed": False, "bits": 6, "iterations": 20,
+         "tolerance": 0.05, "source": "plato/algo/hyperanf/test/test_hyperanf.cc:46-52,133-217"},
+    ],
+    "hyperloglog": [
+        {"test": "add", "bits": 6, "ids": 1000, "max_rel_error": 0.25,
+         "source": "plato/util/test/test_hyperloglog.cc:29-39"},
+        {"test": "merge", "bits": 12, "ids": 1000, "source": "plato/util/test/test_hyperloglog.cc:41-64"},
+    ],
 }
+
+
+def hll_vectors(root: Path) -> dict:
+    """Golden HyperLogLog vectors from the reference's own headers."""
+    import ctypes as C
+    sys.path.insert(0, str(HERE.parent.parent))
+    from oracle.build import build_ref
+    lib = C.CDLL(str(build_ref(ref_root=root)))
+    lib.ref_murmur3_u32.restype = C.c_uint32
+    lib.ref_murmur3_u32.argtypes = [C.c_uint32, C.c_uint32]
+    lib.ref_hll_add.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64]
+    lib.ref_hll_estimate.restype = C.c_double
+    lib.ref_hll_estimate.argtypes = [C.c_uint32, C.c_void_p]
+    rng = np.random.default_rng(20240607)
+    ids = np.concatenate([np.arange(4096, dtype=np.uint32),
+                          rng.integers(0, 2**32, 4096, dtype=np.uint64).astype(np.uint32)])
+    out = {"hash_ids": ids,
+           "hash_values": np.array([lib.ref_murmur3_u32(int(i), 0x5F61767A) for i in ids], np.uint32)}
+    for P in range(4, 17):
+        m = 1 << P
+        rows, ests, counts = [], [], []
+        for n in (1, 7, 100, 3000, 60000):  # ids 0..n-1 added to an empty row
+            r = np.zeros(m, np.uint8)
+            a = np.arange(n, dtype=np.uint32)
+            lib.ref_hll_add(P, r.ctypes.data, a.ctypes.data, n)
+            rows.append(r)
+            counts.append(n)
+            ests.append(lib.ref_hll_estimate(P, r.ctypes.data))
+        for hi in (3, 12, 20):  # random registers: linear counting, raw and large-range branches
+            r = rng.integers(0 if hi < 20 else 14, min(hi, 33 - P) + 1, m).astype(np.uint8)
+            rows.append(r)
+            counts.append(-1)
+            ests.append(lib.ref_hll_estimate(P, r.ctypes.data))
+        out[f"p{P}_rows"] = np.stack(rows)
+        out[f"p{P}_ids"] = np.asarray(counts, np.int64)
+        out[f"p{P}_est"] = np.asarray(ests, np.float64)
+    return out
 
 
 def main(root: Path) -> None:
@@ -78,7 +135,8 @@ def main(root: Path) -> None:
         arrays[f"{key}__dst"] = d
     np.savez_compressed(HERE / "fixtures.npz", **arrays)
     (HERE / "kats.json").write_text(json.dumps(KATS, indent=1) + "\n")
-    print("wrote", HERE / "fixtures.npz", HERE / "kats.json")
+    np.savez_compressed(HERE / "hll_golden.npz", **hll_vectors(root))
+    print("wrote", HERE / "fixtures.npz", HERE / "kats.json", HERE / "hll_golden.npz")
 
 
 if __name__ == "__main__":
