@@ -346,6 +346,7 @@ plato_graph::~plato_graph() {
   plato_b200::destroy_batch_engine(batch_cache);
   plato_b200::destroy_rank_workspace(rank_ws);
   plato_b200::destroy_bfs_workspace(bfs_ws);
+  plato_b200::destroy_hll_workspace(hll_ws);
   if (stream) cudaStreamDestroy(stream);
 }
 

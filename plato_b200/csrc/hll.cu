@@ -47,6 +47,9 @@
 #include <utility>
 #include <vector>
 
+#include <cub/device/device_select.cuh>
+#include <thrust/iterator/counting_iterator.h>
+
 #include "graph.cuh"
 #include "profile.cuh"
 
@@ -57,6 +60,12 @@ constexpr uint32_t kHllSeed = 0x5f61767au;  // hyperloglog.hpp:64
 constexpr int kHllThreads = 256;
 constexpr uint32_t kSumBlocks = 148u * 4u;
 constexpr uint32_t kNoVertex = 0xFFFFFFFFu;
+// Rows with more sources than hub_deg = clamp(kHubBytes / m, kHubMinDeg,
+// kHubMaxDeg) go to the block-per-row kernel (measured on RMAT s22: 2048 at
+// 64-byte rows, 512 from 256-byte rows up).
+constexpr uint32_t kHubBytes = 131072u;
+constexpr uint32_t kHubMinDeg = 512u;
+constexpr uint32_t kHubMaxDeg = 2048u;
 
 __device__ __forceinline__ uint32_t rotl32(uint32_t x, int r) { return (x << r) | (x >> (32 - r)); }
 
@@ -110,9 +119,22 @@ __device__ __forceinline__ bool test_bit(const uint32_t* b, uint32_t v) {
   return (__ldg(b + (v >> 5)) >> (v & 31)) & 1u;
 }
 
-__device__ __forceinline__ uint4 vmax4(uint4 a, uint4 b) {
-  return make_uint4(__vmaxu4(a.x, b.x), __vmaxu4(a.y, b.y), __vmaxu4(a.z, b.z), __vmaxu4(a.w, b.w));
+// Per-byte max of two words whose bytes are below 128 (registers never
+// exceed 33 - P <= 29): bytes where a >= b get a 0x80 flag from a
+// borrow-free subtraction, widened to a byte mask that selects a or b.
+// (Measured on B200 against __vmaxu4: equal or faster at every width.)
+__device__ __forceinline__ uint32_t bmax(uint32_t a, uint32_t b) {
+  const uint32_t d = ((a | 0x80808080u) - b) & 0x80808080u;
+  const uint32_t m = (d - (d >> 7)) | d;
+  return (a & m) | (b & ~m);
 }
+__device__ __forceinline__ uint4 vmax4(uint4 a, uint4 b) {
+  return make_uint4(bmax(a.x, b.x), bmax(a.y, b.y), bmax(a.z, b.z), bmax(a.w, b.w));
+}
+// Even and odd bytes of a word widened to 16-bit lanes, and back.
+__device__ __forceinline__ uint32_t even_bytes(uint32_t w) { return __byte_perm(w, 0u, 0x4240); }
+__device__ __forceinline__ uint32_t odd_bytes(uint32_t w) { return __byte_perm(w, 0u, 0x4341); }
+__device__ __forceinline__ uint32_t join_bytes(uint32_t e, uint32_t o) { return __byte_perm(e, o, 0x6240); }
 
 __device__ __forceinline__ bool differs(uint4 a, uint4 b) {
   return ((a.x ^ b.x) | (a.y ^ b.y) | (a.z ^ b.z) | (a.w ^ b.w)) != 0u;
@@ -151,7 +173,7 @@ struct gather_args {
   uint32_t* changed;          // out: bitmap of rows changed this epoch (zeroed before)
   double* est;                // per-row estimate, rewritten for changed rows
   const uint32_t* fwd_outdeg; // forward out-degree (the engine's switch weight)
-  unsigned long long* counters;  // [0] changed rows, [1] their forward out-degrees
+  unsigned long long* counters;  // [0] changed rows, [1] their forward out-degrees, [2] hub cursor
   const uint32_t* hubs;       // rows with more than hub_deg sources
   uint32_t n_hubs;
   uint32_t V;
@@ -162,68 +184,125 @@ struct gather_args {
   double alpha_mm;
 };
 
-__host__ __device__ constexpr int unroll_for(int vec) { return vec >= 8 ? 1 : 8 / vec; }
+// Source rows in flight per lane (VEC 16-byte words each).
+#ifndef PLATO_HLL_ROWS_IN_FLIGHT
+#define PLATO_HLL_ROWS_IN_FLIGHT 8
+#endif
+__host__ __device__ constexpr int unroll_for(int vec) {
+  return PLATO_HLL_ROWS_IN_FLIGHT / vec < 1 ? 1 : PLATO_HLL_ROWS_IN_FLIGHT / vec;
+}
 
-// Merges the filtered sources adj[c0, e) (team-strided by `stride` ids) of
-// one slice into agg.  Team-uniform control flow; returns whether any source
-// passed the filter.
+// Source ids a team stages per round (in shared memory, after the filter).
+constexpr int kChunk = 32;
+
+// Merges the filtered sources adj[c0, e) of one slice into agg; the team
+// takes kChunk ids per round, rounds `stride` ids apart.  Each round the
+// team's lanes load kChunk / T ids each (the next round's are loaded before
+// this round's rows), keep those that pass the filter compacted in s_ids,
+// then gather their rows UNR at a time.  Team-uniform control flow; returns
+// whether any source passed the filter.
 template <int T, int VEC>
 __device__ __forceinline__ bool team_merge(const gather_args& a, uint64_t c0, uint64_t e,
                                            uint64_t stride, size_t col, int tl, int tb,
-                                           unsigned tmask, uint4 (&agg)[VEC]) {
+                                           unsigned tmask, uint32_t* s_ids, uint4 (&agg)[VEC]) {
+  constexpr int K = kChunk / T;
   constexpr int UNR = unroll_for(VEC);
+  // Up to 2 words per lane, the merge keeps even and odd bytes apart as 16-bit
+  // lanes (__vmaxu2, two per word) and joins them once at the end; wider
+  // slices keep the byte max (the split doubles the accumulator registers).
+  constexpr bool kSplit = VEC <= 2;
   bool any = false;
-  for (uint64_t c = c0; c < e; c += stride) {
-    uint32_t id = kNoVertex;
-    bool ok = false;
-    if (c + tl < e) {
-      id = __ldg(a.adj + c + tl);
-      ok = !a.filter || test_bit(a.filter, id);
-    }
-    unsigned bal = __ballot_sync(tmask, ok) >> tb;
-    any |= bal != 0u;
-    while (bal) {
-      uint32_t src[UNR];
+  uint4 ev[VEC], od[VEC];
 #pragma unroll
-      for (int j = 0; j < UNR; ++j) {
-        const int p = bal ? __ffs(bal) - 1 : 0;
-        const bool has = bal != 0u;
-        bal &= bal - 1u;
-        const uint32_t s = __shfl_sync(tmask, id, tb + p);
-        src[j] = has ? s : kNoVertex;
-      }
+  for (int q = 0; q < VEC; ++q) ev[q] = od[q] = make_uint4(0u, 0u, 0u, 0u);
+  uint32_t nid[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    const uint64_t i = c0 + static_cast<uint64_t>(j) * T + tl;
+    nid[j] = i < e ? __ldg(a.adj + i) : kNoVertex;
+  }
+  for (uint64_t c = c0; c < e; c += stride) {
+    uint32_t ids[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      ids[j] = nid[j];
+      const uint64_t i = c + stride + static_cast<uint64_t>(j) * T + tl;
+      nid[j] = i < e ? __ldg(a.adj + i) : kNoVertex;
+    }
+    uint32_t n = 0;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      const bool ok = ids[j] != kNoVertex && (!a.filter || test_bit(a.filter, ids[j]));
+      const unsigned bal = __ballot_sync(tmask, ok) >> tb;
+      if (ok) s_ids[n + __popc(bal & ((1u << tl) - 1u))] = ids[j];
+      n += __popc(bal);
+    }
+    __syncwarp(tmask);
+    any |= n != 0u;
+    for (uint32_t k = 0; k < n; k += UNR) {
       uint4 r[UNR][VEC];
 #pragma unroll
-      for (int j = 0; j < UNR; ++j)
+      for (int j = 0; j < UNR; ++j) {
+        const bool has = k + j < n;
+        const uint32_t src = has ? s_ids[k + j] : 0u;
 #pragma unroll
         for (int q = 0; q < VEC; ++q)
-          r[j][q] = src[j] != kNoVertex
-                        ? ldg4(a.cur + static_cast<size_t>(src[j]) * a.m + col + q * T * 16)
+          r[j][q] = has ? ldg4(a.cur + static_cast<size_t>(src) * a.m + col + q * T * 16)
                         : make_uint4(0u, 0u, 0u, 0u);
+      }
+      if constexpr (kSplit) {
 #pragma unroll
-      for (int j = 0; j < UNR; ++j)
+        for (int j = 0; j < UNR; ++j)
 #pragma unroll
-        for (int q = 0; q < VEC; ++q) agg[q] = vmax4(agg[q], r[j][q]);
+          for (int q = 0; q < VEC; ++q) {
+            ev[q].x = __vmaxu2(ev[q].x, even_bytes(r[j][q].x));
+            ev[q].y = __vmaxu2(ev[q].y, even_bytes(r[j][q].y));
+            ev[q].z = __vmaxu2(ev[q].z, even_bytes(r[j][q].z));
+            ev[q].w = __vmaxu2(ev[q].w, even_bytes(r[j][q].w));
+            od[q].x = __vmaxu2(od[q].x, odd_bytes(r[j][q].x));
+            od[q].y = __vmaxu2(od[q].y, odd_bytes(r[j][q].y));
+            od[q].z = __vmaxu2(od[q].z, odd_bytes(r[j][q].z));
+            od[q].w = __vmaxu2(od[q].w, odd_bytes(r[j][q].w));
+          }
+      } else {
+#pragma unroll
+        for (int j = 0; j < UNR; ++j)
+#pragma unroll
+          for (int q = 0; q < VEC; ++q) agg[q] = vmax4(agg[q], r[j][q]);
+      }
     }
+    __syncwarp(tmask);  // s_ids is rewritten next round
+  }
+  if constexpr (kSplit) {
+#pragma unroll
+    for (int q = 0; q < VEC; ++q)
+      agg[q] = vmax4(agg[q], make_uint4(join_bytes(ev[q].x, od[q].x), join_bytes(ev[q].y, od[q].y),
+                                        join_bytes(ev[q].z, od[q].z), join_bytes(ev[q].w, od[q].w)));
   }
   return any;
 }
 
-// Applies agg to row v's slice at `col`: nxt = max(cur, agg), written when it
-// changed or the row is stale; accumulates the new slice's register sum.
+template <int T, int VEC>
+__device__ __forceinline__ void load_own(const gather_args& a, uint32_t v, size_t col, uint4 (&own)[VEC]) {
+  const uint8_t* p = a.cur + static_cast<size_t>(v) * a.m + col;
+#pragma unroll
+  for (int q = 0; q < VEC; ++q) own[q] = ldg4(p + q * T * 16);
+}
+
+// Applies agg to row v's slice at `col` (own = its current registers): nxt =
+// max(cur, agg), written when it changed or the row is stale; accumulates the
+// new slice's register sum.
 template <int T, int VEC>
 __device__ __forceinline__ bool team_apply(const gather_args& a, uint32_t v, size_t col, bool stale,
-                                           unsigned tmask, const uint4 (&agg)[VEC],
+                                           unsigned tmask, const uint4 (&own)[VEC], const uint4 (&agg)[VEC],
                                            unsigned long long& sfx, uint32_t& zeros) {
-  const uint8_t* own = a.cur + static_cast<size_t>(v) * a.m + col;
   uint8_t* dst = a.nxt + static_cast<size_t>(v) * a.m + col;
   uint4 nw[VEC];
   bool ch = false;
 #pragma unroll
   for (int q = 0; q < VEC; ++q) {
-    const uint4 o = ldg4(own + q * T * 16);
-    nw[q] = vmax4(o, agg[q]);
-    ch |= differs(o, nw[q]);
+    nw[q] = vmax4(own[q], agg[q]);
+    ch |= differs(own[q], nw[q]);
   }
   ch = __any_sync(tmask, ch);
   if (ch || stale) {
@@ -238,7 +317,7 @@ __device__ __forceinline__ bool team_apply(const gather_args& a, uint32_t v, siz
 // One epoch over the rows with at most hub_deg sources: a team of T lanes per
 // row (grid-strided over rows).
 template <int T, int VEC>
-__global__ void __launch_bounds__(kHllThreads) k_hll_rows(gather_args a) {
+__global__ void __launch_bounds__(kHllThreads, 4) k_hll_rows(gather_args a) {
   constexpr int SLICE = T * VEC * 16;
   const int lane = threadIdx.x & 31;
   const int tl = lane & (T - 1);
@@ -246,11 +325,22 @@ __global__ void __launch_bounds__(kHllThreads) k_hll_rows(gather_args a) {
   const unsigned tmask = T == 32 ? 0xFFFFFFFFu : (((1u << T) - 1u) << tb);
   const uint64_t team = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) / T;
   const uint64_t nteams = static_cast<uint64_t>(gridDim.x) * blockDim.x / T;
+  __shared__ uint32_t s_stage[kHllThreads / T][kChunk];
+  uint32_t* s_ids = s_stage[threadIdx.x / T];
   unsigned long long n_chg = 0, deg_chg = 0;
+  uint64_t nb = 0, ne = 0;
+  if (team < a.V) {
+    nb = __ldg(a.off + team);
+    ne = __ldg(a.off + team + 1);
+  }
   for (uint64_t vv = team; vv < a.V; vv += nteams) {
     const uint32_t v = static_cast<uint32_t>(vv);
+    const uint64_t b = nb, e = ne;
+    if (vv + nteams < a.V) {  // the next row's offsets, one latency early
+      nb = __ldg(a.off + vv + nteams);
+      ne = __ldg(a.off + vv + nteams + 1);
+    }
     if (a.covered && !test_bit(a.covered, v)) continue;
-    const uint64_t b = __ldg(a.off + v), e = __ldg(a.off + v + 1);
     if (e - b > a.hub_deg) continue;
     const bool stale = a.stale && test_bit(a.stale, v);
     bool row_changed = false;
@@ -258,12 +348,16 @@ __global__ void __launch_bounds__(kHllThreads) k_hll_rows(gather_args a) {
     uint32_t zeros = 0;
     for (uint32_t pass = 0; pass < a.passes; ++pass) {
       const size_t col = static_cast<size_t>(pass) * SLICE + static_cast<size_t>(tl) * 16;
-      uint4 agg[VEC];
+      uint4 agg[VEC], own[VEC];
 #pragma unroll
-      for (int q = 0; q < VEC; ++q) agg[q] = make_uint4(0u, 0u, 0u, 0u);
-      const bool any = team_merge<T, VEC>(a, b, e, T, col, tl, tb, tmask, agg);
+      for (int q = 0; q < VEC; ++q) {
+        agg[q] = make_uint4(0u, 0u, 0u, 0u);
+        own[q] = agg[q];
+      }
+      if (e > b || stale) load_own<T, VEC>(a, v, col, own);  // in flight during the merge
+      const bool any = team_merge<T, VEC>(a, b, e, kChunk, col, tl, tb, tmask, s_ids, agg);
       if (!any && !stale) break;  // same scan every pass: nothing to merge, nxt is current
-      row_changed |= team_apply<T, VEC>(a, v, col, stale, tmask, agg, sfx, zeros);
+      row_changed |= team_apply<T, VEC>(a, v, col, stale, tmask, own, agg, sfx, zeros);
     }
     if (row_changed) {
 #pragma unroll
@@ -291,18 +385,28 @@ __global__ void __launch_bounds__(kHllThreads) k_hll_rows(gather_args a) {
 // its kHllThreads / T teams splitting the sources, then a max-reduction over
 // the teams (shuffles inside a warp, shared memory across warps).
 template <int T, int VEC>
-__global__ void __launch_bounds__(kHllThreads) k_hll_hubs(gather_args a) {
+__global__ void __launch_bounds__(kHllThreads, 3) k_hll_hubs(gather_args a) {
   constexpr int SLICE = T * VEC * 16;
   constexpr int kWarps = kHllThreads / 32;
   constexpr int kTeams = kHllThreads / T;
   __shared__ uint4 part[kWarps][T * VEC];
+  __shared__ uint32_t s_stage[kTeams][kChunk];
+  uint32_t* s_ids = s_stage[threadIdx.x / T];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int tl = lane & (T - 1);
   const int tb = lane - tl;
   const unsigned tmask = T == 32 ? 0xFFFFFFFFu : (((1u << T) - 1u) << tb);
-  const uint64_t team_first = static_cast<uint64_t>(threadIdx.x / T) * T;
+  const uint64_t team_first = static_cast<uint64_t>(threadIdx.x / T) * kChunk;
+  __shared__ uint32_t s_next;
   unsigned long long n_chg = 0, deg_chg = 0;
-  for (uint32_t h = blockIdx.x; h < a.n_hubs; h += gridDim.x) {
+  for (;;) {
+    // hubs are listed heaviest first (ascending internal ids); blocks take the
+    // next one as they finish
+    if (threadIdx.x == 0) s_next = atomicAdd(reinterpret_cast<unsigned int*>(a.counters + 2), 1u);
+    __syncthreads();
+    const uint32_t h = s_next;
+    __syncthreads();
+    if (h >= a.n_hubs) break;
     const uint32_t v = a.hubs[h];
     if (a.covered && !test_bit(a.covered, v)) continue;
     const uint64_t b = __ldg(a.off + v), e = __ldg(a.off + v + 1);
@@ -315,8 +419,8 @@ __global__ void __launch_bounds__(kHllThreads) k_hll_hubs(gather_args a) {
       uint4 agg[VEC];
 #pragma unroll
       for (int q = 0; q < VEC; ++q) agg[q] = make_uint4(0u, 0u, 0u, 0u);
-      bool any = team_merge<T, VEC>(a, b + team_first, e, static_cast<uint64_t>(kTeams) * T, col,
-                                    tl, tb, tmask, agg);
+      bool any = team_merge<T, VEC>(a, b + team_first, e, static_cast<uint64_t>(kTeams) * kChunk, col,
+                                    tl, tb, tmask, s_ids, agg);
 #pragma unroll
       for (int o = T; o < 32; o <<= 1)
 #pragma unroll
@@ -335,7 +439,9 @@ __global__ void __launch_bounds__(kHllThreads) k_hll_hubs(gather_args a) {
           for (int w = 1; w < kWarps; ++w) x = vmax4(x, part[w][q * T + tl]);
           agg[q] = x;
         }
-        row_changed |= team_apply<T, VEC>(a, v, col, stale, tmask, agg, sfx, zeros);
+        uint4 own[VEC];
+        load_own<T, VEC>(a, v, col, own);
+        row_changed |= team_apply<T, VEC>(a, v, col, stale, tmask, own, agg, sfx, zeros);
       }
       __syncthreads();  // part is rewritten by the next pass or row
     }
@@ -435,13 +541,13 @@ __global__ void k_bits_weight(const uint32_t* __restrict__ bits, const uint32_t*
   }
 }
 
-// Rows with more than hub_deg sources (order irrelevant: rows are independent).
-__global__ void k_hub_list(const uint64_t* __restrict__ off, uint32_t V, uint32_t hub_deg,
-                           uint32_t* hubs, uint32_t* n_hubs) {
-  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < V;
-       i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-    if (off[i + 1] - off[i] > hub_deg) hubs[atomicAdd(n_hubs, 1u)] = static_cast<uint32_t>(i);
-}
+// Rows with more than hub_deg sources, selected in ascending id order (on a
+// graph relabelled by descending in-degree: heaviest first).
+struct heavy_row {
+  const uint64_t* off;
+  uint32_t hub_deg;
+  __device__ bool operator()(uint32_t v) const { return off[v + 1] - off[v] > hub_deg; }
+};
 
 // Deterministic sum of the estimates: fixed contiguous ranges per block, a
 // fixed reduction tree, then one block over the partials.
@@ -489,17 +595,24 @@ __global__ void k_rows_to_ext(const uint8_t* __restrict__ src, uint8_t* dst,
   }
 }
 
+}  // namespace
+
 // ---------------------------------------------------------------------------
 
-struct direction {
+struct hll_direction {
   const uint64_t* off;
   const uint32_t* adj;
   const uint32_t* hubs;
   uint32_t n_hubs;
 };
 
+// Per-graph HLL state, kept between calls: register buffers (released after
+// a call when they exceed kKeepBytes), estimates, bitmaps, counters and the
+// hub-row lists of both directions.
 class hll_engine {
  public:
+  static constexpr size_t kKeepBytes = 8ull << 30;
+
   explicit hll_engine(plato_graph* g) : g_(g), st_(g->stream), V_(g->info.vertices) {}
 
   int init(uint32_t P) {
@@ -508,31 +621,62 @@ class hll_engine {
     alpha_ = hll_alpha_mm(P);
     const uint32_t slice = P >= 12 ? 4096u : m_;
     passes_ = m_ / slice;
-    hub_deg_ = 131072u / m_ < 32u ? 32u : 131072u / m_;
+    hub_deg_ = std::min(kHubMaxDeg, std::max(kHubMinDeg, kHubBytes / m_));
     const size_t rows = static_cast<size_t>(V_ ? V_ : 1) * m_;
     PLATO_TRY(A_.alloc(rows));
     PLATO_TRY(B_.alloc(rows));
     PLATO_TRY(est_.alloc(V_ ? V_ : 1));
     PLATO_TRY(partial_.alloc(kSumBlocks + 1));
-    PLATO_TRY(ctr_.alloc(2));
+    PLATO_TRY(ctr_.alloc(3));
     words_ = (V_ + 31) / 32;
     for (auto& b : bits_) PLATO_TRY(b.alloc(words_ ? words_ : 1));
-    PLATO_TRY(h_ctr_.alloc(2));
+    for (auto& d : deg_) PLATO_TRY(d.alloc(V_ ? V_ : 1));
+    PLATO_TRY(h_ctr_.alloc(3));
     return PLATO_OK;
   }
 
-  // Hub rows of one direction, listed once per call.
-  int hubs_of(const uint64_t* off, dbuf<uint32_t>& list, uint32_t* n) {
+  // Rows gather their in-neighbours (csr = false) or out-neighbours (csr =
+  // true); the hub rows of each direction are listed once per width class.
+  int direction(bool csr, hll_direction* d) {
+    const int k = csr ? 1 : 0;
+    if (hub_deg_of_[k] != hub_deg_) {
+      PLATO_TRY(list_hubs(csr ? g_->out_off.p : g_->in_off.p, hub_list_[k], &hub_n_[k]));
+      hub_deg_of_[k] = hub_deg_;
+    }
+    *d = hll_direction{csr ? g_->out_off.p : g_->in_off.p, csr ? g_->out_adj.p : g_->in_adj.p,
+                       hub_list_[k].p, hub_n_[k]};
+    return PLATO_OK;
+  }
+
+  // Large register buffers are not kept past the call.
+  void trim() {
+    if (A_.bytes() + B_.bytes() > kKeepBytes) {
+      A_.release();
+      B_.release();
+    }
+  }
+
+  uint32_t* degrees(int i) { return deg_[i].p; }
+
+ private:
+  int list_hubs(const uint64_t* off, dbuf<uint32_t>& list, uint32_t* n) {
     PLATO_TRY(list.alloc(V_ ? V_ : 1));
-    PLATO_CUDA_TRY(cudaMemsetAsync(ctr_.p, 0, sizeof(unsigned long long), st_));
+    *n = 0;
+    if (!V_) return PLATO_OK;
     uint32_t* cnt = reinterpret_cast<uint32_t*>(ctr_.p);
-    k_hub_list<<<grid_for(V_, kHllThreads), kHllThreads, 0, st_>>>(off, V_, hub_deg_, list.p, cnt);
-    PLATO_LAUNCHED("k_hub_list");
+    const thrust::counting_iterator<uint32_t> ids(0);
+    const heavy_row pred{off, hub_deg_};
+    size_t bytes = 0;
+    PLATO_CUDA_TRY(cub::DeviceSelect::If(nullptr, bytes, ids, list.p, cnt, V_, pred, st_));
+    PLATO_TRY(select_tmp_.alloc(bytes ? bytes : 1));
+    PLATO_CUDA_TRY(cub::DeviceSelect::If(select_tmp_.p, bytes, ids, list.p, cnt, V_, pred, st_));
+    count_launch();
     PLATO_CUDA_TRY(cudaMemcpyAsync(n, cnt, sizeof(uint32_t), cudaMemcpyDeviceToHost, st_));
     PLATO_CUDA_TRY(cudaStreamSynchronize(st_));
     return PLATO_OK;
   }
 
+ public:
   int clear_bits(uint32_t* b) {
     PLATO_CUDA_TRY(cudaMemsetAsync(b, 0, 4ull * (words_ ? words_ : 1), st_));
     return PLATO_OK;
@@ -542,7 +686,7 @@ class hll_engine {
     return PLATO_OK;
   }
   int zero_counters() {
-    PLATO_CUDA_TRY(cudaMemsetAsync(ctr_.p, 0, 2 * sizeof(unsigned long long), st_));
+    PLATO_CUDA_TRY(cudaMemsetAsync(ctr_.p, 0, 3 * sizeof(unsigned long long), st_));
     return PLATO_OK;
   }
   int read_counters(unsigned long long* n, unsigned long long* deg) {
@@ -578,7 +722,7 @@ class hll_engine {
 
   // One propagation epoch over `dir`: rows merge their filtered sources.
   // Counters hold the changed rows and their forward out-degrees afterwards.
-  int epoch(const direction& dir, const uint32_t* filter, const uint32_t* covered, const uint32_t* stale,
+  int epoch(const hll_direction& dir, const uint32_t* filter, const uint32_t* covered, const uint32_t* stale,
             uint32_t* changed, unsigned long long* n_changed, unsigned long long* deg_changed) {
     PLATO_TRY(clear_bits(changed));
     PLATO_TRY(zero_counters());
@@ -610,7 +754,7 @@ class hll_engine {
   }
 
   // One spread epoch over `dir` (rows = candidates, sources tested in `active`).
-  int spread(const direction& dir, const uint32_t* active, uint32_t* covered, uint32_t* next,
+  int spread(const hll_direction& dir, const uint32_t* active, uint32_t* covered, uint32_t* next,
              unsigned long long* n, unsigned long long* deg) {
     PLATO_TRY(clear_bits(next));
     PLATO_TRY(zero_counters());
@@ -704,7 +848,12 @@ class hll_engine {
   uint8_t* nxt_ = nullptr;
   dbuf<double> est_, partial_;
   dbuf<unsigned long long> ctr_;
+  dbuf<uint8_t> select_tmp_;
   dbuf<uint32_t> bits_[5];
+  dbuf<uint32_t> deg_[2];
+  dbuf<uint32_t> hub_list_[2];
+  uint32_t hub_n_[2] = {0, 0};
+  uint32_t hub_deg_of_[2] = {0, 0};
   struct pinned {
     unsigned long long* p = nullptr;
     int alloc(size_t n) {
@@ -721,6 +870,20 @@ class hll_engine {
     }
   } h_ctr_;
 };
+
+struct hll_workspace {
+  explicit hll_workspace(plato_graph* g) : eng(g) {}
+  hll_engine eng;
+};
+
+void destroy_hll_workspace(hll_workspace* w) { delete w; }
+
+namespace {
+
+hll_engine& engine_of(plato_graph* g) {
+  if (!g->hll_ws) g->hll_ws = new hll_workspace(g);
+  return g->hll_ws->eng;
+}
 
 void record_mode(plato_run_stats& s, bool push) {
   if (push) {
@@ -750,12 +913,10 @@ int hyperanf_impl(plato_graph* g, const plato_hyperanf_opts* o, const plato_dual
   const uint32_t iterations = o ? o->iteration : 20u;
   const double thr = eo ? eo->push_threshold : 0.05;
   PLATO_TRY(check_bits(P));
-  hll_engine h(g);
+  hll_engine& h = engine_of(g);
   PLATO_TRY(h.init(P));
-  dbuf<uint32_t> hubs;
-  direction in_dir{g->in_off.p, g->in_adj.p, nullptr, 0};
-  PLATO_TRY(h.hubs_of(in_dir.off, hubs, &in_dir.n_hubs));
-  in_dir.hubs = hubs.p;
+  hll_direction in_dir{};
+  PLATO_TRY(h.direction(false, &in_dir));
   PLATO_TRY(h.init_rows(nullptr));
   std::vector<double> anfs;
   double anf = 0.0;
@@ -786,6 +947,7 @@ int hyperanf_impl(plato_graph* g, const plato_hyperanf_opts* o, const plato_dual
   if (n_anfs) *n_anfs = static_cast<uint32_t>(anfs.size());
   if (anfs_out) std::copy(anfs.begin(), anfs.end(), anfs_out);
   if (registers) PLATO_TRY(h.registers_to_host(registers));
+  h.trim();
   if (stats) *stats = st;
   return PLATO_OK;
 }
@@ -801,7 +963,7 @@ int nstep_impl(plato_graph* g, const plato_nstep_opts* o, const plato_dualmode_o
   PLATO_TRY(check_bits(P));
   if (type < PLATO_NSTEP_IN || type > PLATO_NSTEP_BOTH)
     return set_error(PLATO_EINVAL, "nstep degrees: type must be 1 (in), 2 (out) or 3 (both)");
-  hll_engine h(g);
+  hll_engine& h = engine_of(g);
   PLATO_TRY(h.init(P));
   const uint32_t V = h.V();
   const cudaStream_t s = h.stream();
@@ -819,17 +981,13 @@ int nstep_impl(plato_graph* g, const plato_nstep_opts* o, const plato_dualmode_o
     PLATO_CUDA_TRY(cudaMemcpyAsync(target, hb.data(), 4ull * ((V + 31) / 32 ? (V + 31) / 32 : 1),
                                    cudaMemcpyHostToDevice, s));
   }
-  dbuf<uint32_t> hubs_in, hubs_out, d_in, d_out;
-  direction fwd{g->in_off.p, g->in_adj.p, nullptr, 0};   // rows gather their in-neighbours
-  direction rev{g->out_off.p, g->out_adj.p, nullptr, 0}; // rows gather their out-neighbours
-  PLATO_TRY(h.hubs_of(fwd.off, hubs_in, &fwd.n_hubs));
-  fwd.hubs = hubs_in.p;
-  PLATO_TRY(h.hubs_of(rev.off, hubs_out, &rev.n_hubs));
-  rev.hubs = hubs_out.p;
-  PLATO_TRY(d_in.alloc(V ? V : 1));
-  PLATO_TRY(d_out.alloc(V ? V : 1));
-  PLATO_CUDA_TRY(cudaMemsetAsync(d_in.p, 0, 4ull * (V ? V : 1), s));
-  PLATO_CUDA_TRY(cudaMemsetAsync(d_out.p, 0, 4ull * (V ? V : 1), s));
+  hll_direction fwd{}, rev{};
+  PLATO_TRY(h.direction(false, &fwd));  // rows gather their in-neighbours
+  PLATO_TRY(h.direction(true, &rev));   // rows gather their out-neighbours
+  uint32_t* d_in = h.degrees(0);
+  uint32_t* d_out = h.degrees(1);
+  PLATO_CUDA_TRY(cudaMemsetAsync(d_in, 0, 4ull * (V ? V : 1), s));
+  PLATO_CUDA_TRY(cudaMemsetAsync(d_out, 0, 4ull * (V ? V : 1), s));
   const uint64_t E = g->stored_edges;
   plato_run_stats st{};
   uint32_t* covered = h.bits(0);
@@ -849,7 +1007,7 @@ int nstep_impl(plato_graph* g, const plato_nstep_opts* o, const plato_dualmode_o
       const bool push = is_push(ae, E, thr);
       record_mode(st, push);
       // push scatters forward; a reversed pull tests out-neighbours
-      const direction& d = (push || !spread_reversed) ? fwd : rev;
+      const hll_direction& d = (push || !spread_reversed) ? fwd : rev;
       PLATO_TRY(h.spread(d, act, covered, nxt, &actives, &ae));
       std::swap(act, nxt);
     }
@@ -878,20 +1036,21 @@ int nstep_impl(plato_graph* g, const plato_nstep_opts* o, const plato_dualmode_o
 
   const bool want_in = type == PLATO_NSTEP_IN || type == PLATO_NSTEP_BOTH;
   const bool want_out = type == PLATO_NSTEP_OUT || type == PLATO_NSTEP_BOTH;
-  if (want_in) PLATO_TRY(phase(true, d_in.p));
+  if (want_in) PLATO_TRY(phase(true, d_in));
   if (want_out) {
     if (type == PLATO_NSTEP_OUT || opt_directed) {
-      PLATO_TRY(phase(false, d_out.p));
+      PLATO_TRY(phase(false, d_out));
     } else {
       // out = in for every vertex (nstepdegrees.hpp:393-398)
-      PLATO_CUDA_TRY(cudaMemcpyAsync(d_out.p, d_in.p, 4ull * (V ? V : 1), cudaMemcpyDeviceToDevice, s));
+      PLATO_CUDA_TRY(cudaMemcpyAsync(d_out, d_in, 4ull * (V ? V : 1), cudaMemcpyDeviceToDevice, s));
     }
   }
   if (in_degrees && V)
-    PLATO_CUDA_TRY(cudaMemcpyAsync(in_degrees, d_in.p, 4ull * V, cudaMemcpyDeviceToHost, s));
+    PLATO_CUDA_TRY(cudaMemcpyAsync(in_degrees, d_in, 4ull * V, cudaMemcpyDeviceToHost, s));
   if (out_degrees && V)
-    PLATO_CUDA_TRY(cudaMemcpyAsync(out_degrees, d_out.p, 4ull * V, cudaMemcpyDeviceToHost, s));
+    PLATO_CUDA_TRY(cudaMemcpyAsync(out_degrees, d_out, 4ull * V, cudaMemcpyDeviceToHost, s));
   PLATO_CUDA_TRY(cudaStreamSynchronize(s));
+  h.trim();
   if (stats) *stats = st;
   return PLATO_OK;
 }
