@@ -468,6 +468,36 @@ def suite_hll(pb, bits=6):
     return out
 
 
+def suite_wpr(pb):
+    """Weighted PageRank (weighted_pagerank.hpp) on the PageRank graph, RMAT s24
+    ef16 seed 3, with seeded uniform(0.1, 10) weights, 20 epochs (eps 0).
+
+    Algorithmic bytes per epoch: 12E (id, weight, gathered state) + 8(V+1)
+    offsets + 16V (old rank, weight sum, new rank, new state)."""
+    V, s, d = pb.rmat(SCALE, EDGEFACTOR, SEED)
+    w = np.random.default_rng(SEED).uniform(0.1, 10.0, s.size)
+    g = pb.Graph(V, s, d, is_directed=True, weights=w)
+    E = int(s.size)
+    g.weighted_pagerank(ITERATIONS, DAMPING, 0.0)
+    kt = _profiled(pb, ("k_pull_warp_weighted",), lambda: g.weighted_pagerank(ITERATIONS, DAMPING, 0.0))
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        g.weighted_pagerank(ITERATIONS, DAMPING, 0.0)
+        times.append(time.perf_counter() - t0)
+    g.close()
+    ms_k, n_k = kt["k_pull_warp_weighted"]
+    epoch_ms = ms_k / max(n_k, 1)
+    alg = 12 * E + 8 * (V + 1) + 16 * V
+    peak, peak_kind = measured_peak()
+    ms = float(np.median(times)) * 1e3
+    return {"workload": f"wpr_rmat_s{SCALE}_ef{EDGEFACTOR}_seed{SEED}_uniform_weights", "vertices": V, "edges": E,
+            "ms_median": ms, "gteps": E * ITERATIONS / (ms / 1e3) / 1e9,
+            "pull_kernel_ms_per_epoch": epoch_ms, "achieved_gbs": alg / (epoch_ms / 1e3) / 1e9,
+            "frac": alg / (epoch_ms / 1e3) / 1e9 / peak, "peak_source": f"{peak_kind} hbm_gbs",
+            "timing": "host clock around plato_weighted_pagerank (20 epochs, host output), median of 3"}
+
+
 def suite_ppr_single(pb):
     """Single-source PPR on RMAT s24 seed 3 until L1 delta < 1e-7, both engines."""
     V, s, d = pb.rmat(24, 16, 3)
@@ -591,7 +621,8 @@ def run_suite(args):
     import torch  # noqa: F401  (CUDA context for the library)
     import plato_b200 as pb
     res = {"suite": True}
-    for name, fn in (("bfs", suite_bfs), ("cc", suite_cc), ("hll", suite_hll), ("ppr_single", suite_ppr_single),
+    for name, fn in (("bfs", suite_bfs), ("cc", suite_cc), ("hll", suite_hll), ("wpr", suite_wpr),
+                     ("ppr_single", suite_ppr_single),
                      ("ppr_batch", suite_batch), ("serving", suite_serving)):
         if args.only and name not in args.only.split(","):
             continue
@@ -613,7 +644,7 @@ def main():
                     help="RMAT scale (smaller values are for profiling captures only)")
     ap.add_argument("--suite", action="store_true",
                     help="also measure BFS, single PPR, batched PPR and serving (one JSON line each)")
-    ap.add_argument("--only", default="", help="with --suite: comma list of bfs,cc,hll,ppr_single,ppr_batch,serving")
+    ap.add_argument("--only", default="", help="with --suite: comma list of bfs,cc,hll,wpr,ppr_single,ppr_batch,serving")
     ap.add_argument("--quick", action="store_true", help="with --suite: one small batch (profiling)")
     args = ap.parse_args()
     globals()["SCALE"] = args.scale

@@ -144,6 +144,14 @@ int plato_profile_read(const char* kernel, double* total_ms, uint64_t* launches)
  * arrays src/dst hold info->edges entries.  Ids >= info->vertices -> EINVAL. */
 int plato_graph_create(const plato_graph_info* info, const plato_vid_t* src,
                        const plato_vid_t* dst, uint32_t flags, plato_graph** out);
+/* Same with a double weight per input edge (create_dcsc_seqs_from_path<double>
+ * with double_decoder, as example/pagerank_weighted.cc:71-74 loads weighted
+ * graphs): each edge keeps its weight (float) in the CSC, and every vertex
+ * the sum of its out-edge weights (summed in double, in CSR row order).
+ * weights: host [info->edges], input order. */
+int plato_graph_create_weighted(const plato_graph_info* info, const plato_vid_t* src,
+                                const plato_vid_t* dst, const double* weights, uint32_t flags,
+                                plato_graph** out);
 int plato_graph_destroy(plato_graph* g);
 int plato_graph_get_info(const plato_graph* g, plato_graph_info* info);
 int plato_graph_get_device_view(const plato_graph* g, plato_graph_device_view* view);
@@ -186,6 +194,14 @@ typedef struct {
  * by zero). */
 int plato_trustrank(plato_graph* g, const plato_trustrank_opts* opts, const uint8_t* good_vertices,
                     float* ranks, plato_vid_t* seeds_out, uint32_t* n_seeds, plato_run_stats* stats);
+/* algo::weighted_pagerank (plato/algo/pagerank/weighted_pagerank.hpp:60-149)
+ * on a graph made by plato_graph_create_weighted (else PLATO_EINVAL): ranks
+ * start at 1, rank' = 1 - d + d * sum of rank[u] * w / weight_sum[u] over
+ * in-edges; eps > 0 and the epoch's sum |rank' - rank| < eps jumps to the last
+ * epoch.  ranks: host [V], caller ids, in the reference's units (not
+ * normalised).  stats->delta = the last delta read (eps > 0). */
+int plato_weighted_pagerank(plato_graph* g, const plato_pagerank_opts* opts, float* ranks,
+                            plato_run_stats* stats);
 /* algo::breadth_first_search (plato/algo/bfs/bfs.hpp:55-155) with the engine's
  * push/pull switch (dualmode.hpp:245-297).  levels/parents: host [V] or NULL. */
 int plato_bfs(plato_graph* g, const plato_bfs_opts* opts, const plato_dualmode_opts* engine_opts,
@@ -361,6 +377,13 @@ int plato_edge_list_free(plato_edge_list* el);
  *          distinct-id count on the compact ids it requires).
  * The result feeds plato_graph_create like an RMAT list. */
 int plato_edge_list_read_csv(const char* path, plato_edge_list** out);
+/* As plato_edge_list_read_csv for weighted edges (csv_parser with
+ * double_decoder, parsers.hpp:84-88, 226-290): a line needs a third field,
+ * read as strtod reads it; lines without one are skipped. */
+int plato_edge_list_read_csv_weighted(const char* path, plato_edge_list** out);
+/* Weights of a weighted list in edge order (valid until plato_edge_list_free),
+ * NULL for an unweighted list. */
+int plato_edge_list_weights(const plato_edge_list* el, const double** weights);
 
 /* Per-vertex results as CSV, the layout the reference's examples write
  * (example/pagerank.cc:191-200, plato/util/foutput.cc:95-101):

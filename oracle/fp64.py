@@ -147,3 +147,39 @@ def cc_components_bfs(vertices: int, src, dst) -> np.ndarray:
                     label[v] = i
                     q.append(v)
     return label.astype(np.uint32)
+
+
+def weighted_pagerank(vertices: int, src, dst, weights, is_directed=True, iterations=100, damping=0.85,
+                      eps=0.001):
+    """algo::weighted_pagerank (plato/algo/pagerank/weighted_pagerank.hpp:60-149)
+    in double: v_weight_sum[u] = sum of u's out-edge weights (:86-99), ranks
+    start at 1 (:104-109); each epoch rank'(v) = 1 - d + d * sum over in-edges
+    (u, v, w) of rank[u] * w / v_weight_sum[u] (:112-130); delta = sum
+    |rank' - rank| except in the last epoch, and eps > 0 with delta < eps
+    jumps to the last epoch (:131-137).  Undirected edges count both ways.
+    Returns (ranks, epochs run, last delta)."""
+    src = np.asarray(src, dtype=np.int64)
+    dst = np.asarray(dst, dtype=np.int64)
+    w = np.asarray(weights, dtype=np.float64)
+    if not is_directed:
+        src, dst, w = np.concatenate([src, dst]), np.concatenate([dst, src]), np.concatenate([w, w])
+    wsum = np.zeros(vertices)
+    np.add.at(wsum, src, w)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        beta = w / wsum[src]
+    A = sp.csr_matrix((beta, (dst, src)), shape=(vertices, vertices))
+    rank = np.ones(vertices)
+    epochs, delta = 0, 0.0
+    epoch = 0
+    while epoch < iterations:
+        nxt = (1.0 - damping) + damping * (A @ rank)
+        epochs += 1
+        if epoch == iterations - 1:
+            rank = nxt
+            break
+        delta = float(np.abs(nxt - rank).sum())
+        rank = nxt
+        if eps > 0.0 and delta < eps:
+            epoch = iterations - 2
+        epoch += 1
+    return rank, epochs, delta

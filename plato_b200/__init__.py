@@ -99,7 +99,7 @@ def _ptr(a: np.ndarray) -> C.c_void_p:
     return C.c_void_p(a.ctypes.data)
 
 
-def _take_edge_list(lib, h):
+def _take_edge_list(lib, h, weighted: bool = False):
     """Copies an edge-list handle into numpy arrays and frees it."""
     try:
         V = C.c_uint32()
@@ -113,7 +113,14 @@ def _take_edge_list(lib, h):
         if n:
             C.memmove(src.ctypes.data, ps.value, 4 * n)
             C.memmove(dst.ctypes.data, pd.value, 4 * n)
-        return int(V.value), src, dst
+        if not weighted:
+            return int(V.value), src, dst
+        pw = C.c_void_p()
+        check(lib.plato_edge_list_weights(h, C.byref(pw)), "plato_edge_list_weights")
+        w = np.empty(n, dtype=np.float64)
+        if n:
+            C.memmove(w.ctypes.data, pw.value, 8 * n)
+        return int(V.value), src, dst, w
     finally:
         lib.plato_edge_list_free(h)
 
@@ -131,14 +138,17 @@ def rmat(scale: int, edgefactor: int = 16, seed: int = 1, a: float = 0.57, b: fl
     return _take_edge_list(lib, h)
 
 
-def read_csv(path) -> tuple:
-    """Edge list from CSV text -> (V, src, dst), the reference's csv_parser
-    rules (plato/graph/parsers.hpp:226-290): `path` is a file or a directory
-    of files (read in name order, ".gz" inflated); V = largest id + 1."""
+def read_csv(path, weighted: bool = False) -> tuple:
+    """Edge list from CSV text -> (V, src, dst), or (V, src, dst, weights
+    float64) when weighted, the reference's csv_parser rules
+    (plato/graph/parsers.hpp:226-290; weights with double_decoder, :84-88):
+    `path` is a file or a directory of files (read in name order, ".gz"
+    inflated); V = largest id + 1."""
     lib = load()
     h = C.c_void_p()
-    check(lib.plato_edge_list_read_csv(os.fsencode(str(path)), C.byref(h)), "plato_edge_list_read_csv")
-    return _take_edge_list(lib, h)
+    fn = lib.plato_edge_list_read_csv_weighted if weighted else lib.plato_edge_list_read_csv
+    check(fn(os.fsencode(str(path)), C.byref(h)), "plato_edge_list_read_csv")
+    return _take_edge_list(lib, h, weighted)
 
 
 def write_vertex_csv(directory, values, prefix: str = "", files: int = 1, gzip: bool = False) -> None:
@@ -163,7 +173,8 @@ class Graph:
     for an in-memory edge list.  ``relabel`` lets the engine renumber vertices
     internally by out-degree; results always come back in caller ids."""
 
-    def __init__(self, vertices: int, src, dst, is_directed: bool = True, relabel: bool = True):
+    def __init__(self, vertices: int, src, dst, is_directed: bool = True, relabel: bool = True,
+                 weights=None):
         self._lib = load()
         src = _u32(src)
         dst = _u32(dst)
@@ -172,9 +183,16 @@ class Graph:
         info = _lib.GraphInfo(1 if is_directed else 0, int(vertices), int(src.size),
                               max(int(vertices) - 1, 0))
         h = C.c_void_p()
-        check(self._lib.plato_graph_create(C.byref(info), _ptr(src), _ptr(dst),
-                                           PLATO_GRAPH_RELABEL if relabel else 0, C.byref(h)),
-              "plato_graph_create")
+        flags = PLATO_GRAPH_RELABEL if relabel else 0
+        if weights is None:
+            check(self._lib.plato_graph_create(C.byref(info), _ptr(src), _ptr(dst), flags, C.byref(h)),
+                  "plato_graph_create")
+        else:
+            w = np.ascontiguousarray(weights, dtype=np.float64)
+            if w.shape != src.shape:
+                raise ValueError("weights must have one entry per edge")
+            check(self._lib.plato_graph_create_weighted(C.byref(info), _ptr(src), _ptr(dst), _ptr(w), flags,
+                                                        C.byref(h)), "plato_graph_create_weighted")
         self._h = h
 
     # -- lifetime ---------------------------------------------------------
@@ -247,6 +265,17 @@ class Graph:
                                               C.c_void_p(stream), C.byref(s)),
               "plato_pagerank_device")
         return RunStats.from_c(s)
+
+    def weighted_pagerank(self, iteration: int = 100, damping: float = 0.85, eps: float = 0.001):
+        """algo::weighted_pagerank (plato/algo/pagerank/weighted_pagerank.hpp:60-149)
+        on a graph built with weights -> (ranks float32 [V] in the reference's
+        units, stats)."""
+        out = np.empty(self.vertices, dtype=np.float32)
+        o = _lib.PagerankOpts(iteration, damping, eps)
+        s = _lib.RunStats()
+        check(self._lib.plato_weighted_pagerank(self.handle, C.byref(o), _ptr(out), C.byref(s)),
+              "plato_weighted_pagerank")
+        return out, RunStats.from_c(s)
 
     def personalized_pagerank(self, src: int, iteration: int = 100, damping: float = 0.85,
                               eps: float = 0.0, mode: int = PLATO_PPR_PULL):

@@ -105,6 +105,8 @@ SIGNATURES = {
     "plato_profile_reset": (C.c_int, []),
     "plato_profile_read": (C.c_int, [C.c_char_p, C.POINTER(C.c_double), u64p]),
     "plato_graph_create": (C.c_int, [C.POINTER(GraphInfo), P, P, C.c_uint32, C.POINTER(P)]),
+    "plato_graph_create_weighted": (C.c_int, [C.POINTER(GraphInfo), P, P, P, C.c_uint32, C.POINTER(P)]),
+    "plato_weighted_pagerank": (C.c_int, [P, C.POINTER(PagerankOpts), P, C.POINTER(RunStats)]),
     "plato_graph_destroy": (C.c_int, [P]),
     "plato_graph_get_info": (C.c_int, [P, C.POINTER(GraphInfo)]),
     "plato_graph_get_device_view": (C.c_int, [P, C.POINTER(GraphDeviceView)]),
@@ -138,6 +140,8 @@ SIGNATURES = {
     "plato_edge_list_data": (C.c_int, [P, C.POINTER(P), C.POINTER(P)]),
     "plato_edge_list_free": (C.c_int, [P]),
     "plato_edge_list_read_csv": (C.c_int, [C.c_char_p, C.POINTER(P)]),
+    "plato_edge_list_read_csv_weighted": (C.c_int, [C.c_char_p, C.POINTER(P)]),
+    "plato_edge_list_weights": (C.c_int, [P, C.POINTER(P)]),
     "plato_write_vertex_csv": (C.c_int, [C.c_char_p, C.c_char_p, P, C.c_int, C.c_uint32, C.c_uint32,
                                          C.c_int]),
 }

@@ -10,4 +10,6 @@ struct plato_edge_list {
   plato_vid_t vertices = 0;
   std::vector<plato_vid_t> src;
   std::vector<plato_vid_t> dst;
+  bool weighted = false;
+  std::vector<double> w;  // weighted lists: one weight per edge
 };

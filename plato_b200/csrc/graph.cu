@@ -15,6 +15,13 @@
 // power-law graphs the most-gathered rank values share cache lines at the
 // front of the rank vector; to_int/to_ext map between the numberings.  Adjacency lists are sorted
 // ascending, so the graph is a pure function of the edge multiset.
+//
+// Weighted graphs (create_dcsc_seqs_from_path<double>, structure.hpp, as
+// example/pagerank_weighted.cc:71-74 loads them) carry each edge's double
+// weight through the same stable sorts: the CSC keeps a float weight per
+// edge (in_w), the CSR side yields each vertex's sum of out-edge weights
+// (out_wsum, summed in double per row, in row order, then rounded), the
+// v_weight_sum of weighted_pagerank.hpp:86-99.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -77,6 +84,22 @@ __global__ void k_edge_keys(const uint32_t* __restrict__ src, const uint32_t* __
     keys[i] = (major << shift) | minor;
     if (undirected) keys[n + i] = (minor << shift) | major;
   }
+}
+
+// Weights follow their edge keys: vals[i] = w[i], and vals[n + i] = w[i] for
+// the reversed copy of an undirected edge.
+__global__ void k_edge_vals(const double* __restrict__ w, uint64_t n, int undirected, double* vals) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    vals[i] = w[i];
+    if (undirected) vals[n + i] = w[i];
+  }
+}
+
+__global__ void k_to_float(const double* __restrict__ in, uint64_t n, float* out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = static_cast<float>(in[i]);
 }
 
 __global__ void k_keys_to_adj(const uint64_t* __restrict__ keys, uint64_t n, uint64_t mask,
@@ -154,6 +177,23 @@ int radix_sort(uint64_t* a, uint64_t* b, uint64_t n, int end_bit, dbuf<uint8_t>&
   return PLATO_OK;
 }
 
+// Stable key sort carrying double values.
+int radix_sort_pairs(uint64_t* ka, uint64_t* kb, double* va, double* vb, uint64_t n, int end_bit,
+                     dbuf<uint8_t>& tmp, cudaStream_t st, uint64_t** sk, double** sv) {
+  cub::DoubleBuffer<uint64_t> dk(ka, kb);
+  cub::DoubleBuffer<double> dv(va, vb);
+  size_t bytes = 0;
+  PLATO_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, bytes, dk, dv, static_cast<int64_t>(n), 0,
+                                                 end_bit, st));
+  PLATO_TRY(tmp.alloc(bytes));
+  PLATO_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp.p, bytes, dk, dv, static_cast<int64_t>(n), 0,
+                                                 end_bit, st));
+  count_launch();
+  *sk = dk.Current();
+  *sv = dv.Current();
+  return PLATO_OK;
+}
+
 int exclusive_scan_u64(const uint64_t* in, uint64_t* out, uint64_t n, dbuf<uint8_t>& tmp,
                        cudaStream_t st) {
   size_t bytes = 0;
@@ -164,10 +204,21 @@ int exclusive_scan_u64(const uint64_t* in, uint64_t* out, uint64_t n, dbuf<uint8
   return PLATO_OK;
 }
 
+// Edge weights of one side (weighted graphs): the sorted values are kept
+// per edge (edge_w, the CSC) or summed per row (row_wsum, the CSR).
+struct side_weights {
+  const double* w = nullptr;  // input order, device
+  dbuf<double>* va = nullptr;
+  dbuf<double>* vb = nullptr;
+  dbuf<float>* edge_w = nullptr;
+  dbuf<float>* row_wsum = nullptr;
+};
+
 int build_side(plato_graph* g, const dbuf<uint32_t>& d_src, const dbuf<uint32_t>& d_dst,
                const dbuf<uint32_t>& deg_ext, bool by_dst, dbuf<uint64_t>& keys_a,
                dbuf<uint64_t>& keys_b, dbuf<uint8_t>& tmp, dbuf<uint64_t>& off,
-               dbuf<uint32_t>& adj, dbuf<uint32_t>* deg_int, cudaStream_t st) {
+               dbuf<uint32_t>& adj, dbuf<uint32_t>* deg_int, cudaStream_t st,
+               const side_weights& sw = side_weights()) {
   const uint32_t V = g->info.vertices;
   const uint64_t n = g->info.edges;
   const uint64_t E = g->stored_edges;
@@ -178,7 +229,17 @@ int build_side(plato_graph* g, const dbuf<uint32_t>& d_src, const dbuf<uint32_t>
                                                  by_dst ? 1 : 0, keys_a.p);
   PLATO_LAUNCHED("k_edge_keys");
   uint64_t* sorted = keys_a.p;
-  if (E > 1) PLATO_TRY(radix_sort(keys_a.p, keys_b.p, E, 2 * shift, tmp, st, &sorted));
+  double* sorted_w = nullptr;
+  if (sw.w) {
+    k_edge_vals<<<grid_for(n, 256), 256, 0, st>>>(sw.w, n, undirected, sw.va->p);
+    PLATO_LAUNCHED("k_edge_vals");
+    sorted_w = sw.va->p;
+    if (E > 1)
+      PLATO_TRY(radix_sort_pairs(keys_a.p, keys_b.p, sw.va->p, sw.vb->p, E, 2 * shift, tmp, st, &sorted,
+                                 &sorted_w));
+  } else if (E > 1) {
+    PLATO_TRY(radix_sort(keys_a.p, keys_b.p, E, 2 * shift, tmp, st, &sorted));
+  }
   PLATO_TRY(adj.alloc(E > 0 ? E : 1));
   k_keys_to_adj<<<grid_for(E, 256), 256, 0, st>>>(sorted, E, (1ull << shift) - 1, adj.p);
   PLATO_LAUNCHED("k_keys_to_adj");
@@ -192,11 +253,34 @@ int build_side(plato_graph* g, const dbuf<uint32_t>& d_src, const dbuf<uint32_t>
   PLATO_LAUNCHED("k_internal_degrees");
   PLATO_TRY(off.alloc(static_cast<size_t>(V) + 1));
   PLATO_TRY(exclusive_scan_u64(deg64.p, off.p, static_cast<uint64_t>(V) + 1, tmp, st));
+  if (sw.edge_w) {
+    PLATO_TRY(sw.edge_w->alloc(E > 0 ? E : 1));
+    if (E > 0) {
+      k_to_float<<<grid_for(E, 256), 256, 0, st>>>(sorted_w, E, sw.edge_w->p);
+      PLATO_LAUNCHED("k_to_float");
+    }
+  }
+  if (sw.row_wsum) {
+    // per-row sums in double (a fixed reduction per segment), then float
+    dbuf<double> sums;
+    PLATO_TRY(sums.alloc(V));
+    size_t bytes = 0;
+    PLATO_CUDA_TRY(cub::DeviceSegmentedReduce::Sum(nullptr, bytes, sorted_w, sums.p, static_cast<int64_t>(V),
+                                                   off.p, off.p + 1, st));
+    PLATO_TRY(tmp.alloc(bytes));
+    PLATO_CUDA_TRY(cub::DeviceSegmentedReduce::Sum(tmp.p, bytes, sorted_w, sums.p, static_cast<int64_t>(V),
+                                                   off.p, off.p + 1, st));
+    count_launch();
+    PLATO_TRY(sw.row_wsum->alloc(V));
+    k_to_float<<<grid_for(V, 256), 256, 0, st>>>(sums.p, V, sw.row_wsum->p);
+    PLATO_LAUNCHED("k_to_float");
+    PLATO_CUDA_TRY(cudaStreamSynchronize(st));  // sums is freed on return
+  }
   return PLATO_OK;
 }
 
 int create_impl(const plato_graph_info* info, const uint32_t* src, const uint32_t* dst,
-                uint32_t flags, plato_graph* g) {
+                const double* weights, uint32_t flags, plato_graph* g) {
   g->info = *info;
   g->info.max_v_i = info->vertices > 0 ? info->vertices - 1 : 0;
   const uint32_t V = info->vertices;
@@ -254,10 +338,22 @@ int create_impl(const plato_graph_info* info, const uint32_t* src, const uint32_
     dbuf<uint64_t> keys_a, keys_b;
     PLATO_TRY(keys_a.alloc(E > 0 ? E : 1));
     PLATO_TRY(keys_b.alloc(E > 0 ? E : 1));
+    dbuf<double> d_w, va, vb;
+    side_weights in_sw, out_sw;
+    if (weights) {
+      g->weighted = true;
+      PLATO_TRY(d_w.alloc(n > 0 ? n : 1));
+      PLATO_TRY(va.alloc(E > 0 ? E : 1));
+      PLATO_TRY(vb.alloc(E > 0 ? E : 1));
+      if (n > 0)
+        PLATO_CUDA_TRY(cudaMemcpyAsync(d_w.p, weights, n * sizeof(double), cudaMemcpyHostToDevice, st));
+      in_sw = side_weights{d_w.p, &va, &vb, &g->in_w, nullptr};
+      out_sw = side_weights{d_w.p, &va, &vb, nullptr, &g->out_wsum};
+    }
     PLATO_TRY(build_side(g, d_src, d_dst, deg_in_ext, true, keys_a, keys_b, tmp, g->in_off,
-                         g->in_adj, &g->in_deg, st));
+                         g->in_adj, &g->in_deg, st, in_sw));
     PLATO_TRY(build_side(g, d_src, d_dst, deg_out_ext, false, keys_a, keys_b, tmp, g->out_off,
-                         g->out_adj, &g->out_deg, st));
+                         g->out_adj, &g->out_deg, st, out_sw));
     PLATO_CUDA_TRY(cudaStreamSynchronize(st));
   }
   return PLATO_OK;
@@ -347,27 +443,46 @@ plato_graph::~plato_graph() {
   plato_b200::destroy_rank_workspace(rank_ws);
   plato_b200::destroy_bfs_workspace(bfs_ws);
   plato_b200::destroy_hll_workspace(hll_ws);
+  plato_b200::destroy_wpr_workspace(wpr_ws);
   if (stream) cudaStreamDestroy(stream);
 }
 
 using namespace plato_b200;
 
-extern "C" int plato_graph_create(const plato_graph_info* info, const plato_vid_t* src,
-                                  const plato_vid_t* dst, uint32_t flags, plato_graph** out) {
-  if (!info || !out) return set_error(PLATO_EINVAL, "plato_graph_create: null argument");
+namespace {
+
+int create_checked(const plato_graph_info* info, const plato_vid_t* src, const plato_vid_t* dst,
+                   const double* weights, uint32_t flags, plato_graph** out, const char* who) {
+  if (!info || !out) return set_error(PLATO_EINVAL, std::string(who) + ": null argument");
   *out = nullptr;
   if (info->edges > 0 && (!src || !dst))
-    return set_error(PLATO_EINVAL, "plato_graph_create: null edge arrays");
-  if (info->vertices == 0) return set_error(PLATO_EINVAL, "plato_graph_create: zero vertices");
+    return set_error(PLATO_EINVAL, std::string(who) + ": null edge arrays");
+  if (info->vertices == 0) return set_error(PLATO_EINVAL, std::string(who) + ": zero vertices");
   plato_graph* g = new (std::nothrow) plato_graph();
-  if (!g) return set_error(PLATO_ENOMEM, "plato_graph_create: host allocation failed");
-  const int s = create_impl(info, src, dst, flags, g);
+  if (!g) return set_error(PLATO_ENOMEM, std::string(who) + ": host allocation failed");
+  const int s = create_impl(info, src, dst, weights, flags, g);
   if (s != PLATO_OK) {
     delete g;
     return s;
   }
   *out = g;
   return PLATO_OK;
+}
+
+}  // namespace
+
+extern "C" int plato_graph_create(const plato_graph_info* info, const plato_vid_t* src,
+                                  const plato_vid_t* dst, uint32_t flags, plato_graph** out) {
+  return create_checked(info, src, dst, nullptr, flags, out, "plato_graph_create");
+}
+
+extern "C" int plato_graph_create_weighted(const plato_graph_info* info, const plato_vid_t* src,
+                                           const plato_vid_t* dst, const double* weights, uint32_t flags,
+                                           plato_graph** out) {
+  if (info && info->edges > 0 && !weights)
+    return set_error(PLATO_EINVAL, "plato_graph_create_weighted: null weights");
+  static const double kNone = 0.0;
+  return create_checked(info, src, dst, weights ? weights : &kNone, flags, out, "plato_graph_create_weighted");
 }
 
 extern "C" int plato_graph_destroy(plato_graph* g) {
@@ -417,6 +532,7 @@ extern "C" int plato_graph_out_degrees(plato_graph* g, uint32_t* degrees_out) {
 extern "C" int plato_graph_device_bytes(const plato_graph* g, uint64_t* bytes) {
   if (!g || !bytes) return set_error(PLATO_EINVAL, "plato_graph_device_bytes: null argument");
   *bytes = g->in_off.bytes() + g->out_off.bytes() + g->in_adj.bytes() + g->out_adj.bytes() +
-           g->out_deg.bytes() + g->in_deg.bytes() + g->to_int.bytes() + g->to_ext.bytes();
+           g->out_deg.bytes() + g->in_deg.bytes() + g->to_int.bytes() + g->to_ext.bytes() +
+           g->in_w.bytes() + g->out_wsum.bytes();
   return PLATO_OK;
 }

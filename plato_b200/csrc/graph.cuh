@@ -25,9 +25,11 @@ struct rank_workspace;   // rank.cu
 struct bfs_workspace;    // bfs.cu
 class batch_engine;      // ppr_batch.cu
 struct hll_workspace;    // hll.cu
+struct wpr_workspace;    // wpagerank.cu
 void destroy_rank_workspace(rank_workspace*);
 void destroy_bfs_workspace(bfs_workspace*);
 void destroy_hll_workspace(hll_workspace*);
+void destroy_wpr_workspace(wpr_workspace*);
 void destroy_batch_engine(batch_engine*);
 
 }  // namespace plato_b200
@@ -42,6 +44,9 @@ struct plato_graph {
   plato_b200::dbuf<uint32_t> in_adj, out_adj;
   plato_b200::dbuf<uint32_t> out_deg, in_deg;
   plato_b200::dbuf<uint32_t> to_int, to_ext;  // empty when not relabeled
+  bool weighted = false;
+  plato_b200::dbuf<float> in_w;      // [E] weight of each CSC edge (weighted graphs)
+  plato_b200::dbuf<float> out_wsum;  // [V] sum of each vertex's out-edge weights
 
   cudaStream_t stream = nullptr;  // stream of the host-buffer entry points
   std::mutex mu;                  // one algorithm call at a time per graph
@@ -50,6 +55,7 @@ struct plato_graph {
   plato_b200::rank_workspace* rank_ws = nullptr;
   plato_b200::bfs_workspace* bfs_ws = nullptr;
   plato_b200::hll_workspace* hll_ws = nullptr;  // HyperLogLog buffers (hll.cu)
+  plato_b200::wpr_workspace* wpr_ws = nullptr;  // weighted PageRank buffers (wpagerank.cu)
   plato_b200::batch_engine* batch_cache = nullptr;  // plato_ppr_batch state, kept between calls
   std::vector<uint32_t> h_to_int;             // host copy of to_int (lazily)
   std::map<uint32_t, uint32_t> batch_tuned;   // K bucket -> columns per tile (kt)

@@ -13,6 +13,9 @@
 //           decimal digits up to the first other character; no digits -> 0).
 //           Empty lines and lines without a second field are skipped.  A
 //           value above 2^32 - 1 is an error here (the reference aborts).
+//           Weighted lists (double_decoder, parsers.hpp:84-88) also need a
+//           third field, read as strtod reads it (the field alone, as strtok
+//           cuts it); lines without one are skipped.
 //   info    edges = lines parsed; vertices = largest id + 1.  The reference
 //           counts distinct ids and requires them compact
 //           (plato/graph/structure.hpp:199-232, dcsc.hpp:48-49), so the two
@@ -71,8 +74,19 @@ bool read_id(const char* p, const char* e, uint32_t* out) {
   return true;
 }
 
+// strtod on the field [p, e) alone.
+double read_weight(const char* p, const char* e) {
+  char tmp[64];
+  const size_t n = std::min<size_t>(static_cast<size_t>(e - p), sizeof(tmp) - 1);
+  std::memcpy(tmp, p, n);
+  tmp[n] = '\0';
+  if (static_cast<size_t>(e - p) < sizeof(tmp)) return std::strtod(tmp, nullptr);
+  return std::strtod(std::string(p, e).c_str(), nullptr);
+}
+
 // One line [b, e) without its '\n'.  1 = edge, 0 = skipped, -1 = id too large.
-int parse_line(const char* b, const char* e, uint32_t* s, uint32_t* d) {
+// w non-null: the line needs a third field (the weight).
+int parse_line(const char* b, const char* e, uint32_t* s, uint32_t* d, double* w = nullptr) {
   if (b == e) return 0;
   const char* p = b;
   while (p < e && *p == ',') ++p;  // strtok: leading delimiters
@@ -85,6 +99,13 @@ int parse_line(const char* b, const char* e, uint32_t* s, uint32_t* d) {
   const char* f2 = p;
   while (p < e && *p != ',') ++p;
   if (!read_id(f1, f1e, s) || !read_id(f2, p, d)) return -1;
+  if (w) {
+    while (p < e && *p == ',') ++p;
+    if (p == e) return 0;  // no weight field: the decoder fails, the line is skipped
+    const char* f3 = p;
+    while (p < e && *p != ',') ++p;
+    *w = read_weight(f3, p);
+  }
   return 1;
 }
 
@@ -122,9 +143,9 @@ int read_whole(const std::string& name, std::string* buf) {
   return PLATO_OK;
 }
 
-// Parses one file's text, appending to src/dst in line order.
+// Parses one file's text, appending to src/dst (and w when weighted) in line order.
 int parse_buffer(const std::string& buf, const std::string& name, std::vector<uint32_t>& src,
-                 std::vector<uint32_t>& dst) {
+                 std::vector<uint32_t>& dst, std::vector<double>* wts = nullptr) {
   const size_t n = buf.size();
   const int T = std::max(1, std::min(omp_get_max_threads(), static_cast<int>(n / (1 << 20)) + 1));
   std::vector<size_t> cut(T + 1, n);
@@ -135,6 +156,7 @@ int parse_buffer(const std::string& buf, const std::string& name, std::vector<ui
     cut[t] = p;
   }
   std::vector<std::vector<uint32_t>> ls(T), ld(T);
+  std::vector<std::vector<double>> lw(T);
   std::vector<long long> bad(T, -1);  // first offending line start per piece
 #pragma omp parallel for num_threads(T) schedule(static, 1)
   for (int t = 0; t < T; ++t) {
@@ -147,10 +169,12 @@ int parse_buffer(const std::string& buf, const std::string& name, std::vector<ui
       const char* nl = static_cast<const char*>(std::memchr(base + p, '\n', end - p));
       const size_t le = nl ? static_cast<size_t>(nl - base) : end;
       uint32_t s = 0, d = 0;
-      const int r = parse_line(base + p, base + le, &s, &d);
+      double w = 0.0;
+      const int r = parse_line(base + p, base + le, &s, &d, wts ? &w : nullptr);
       if (r == 1) {
         ls[t].push_back(s);
         ld[t].push_back(d);
+        if (wts) lw[t].push_back(w);
       } else if (r < 0 && bad[t] < 0) {
         bad[t] = static_cast<long long>(p);
       }
@@ -166,6 +190,7 @@ int parse_buffer(const std::string& buf, const std::string& name, std::vector<ui
   for (int t = 0; t < T; ++t) {
     src.insert(src.end(), ls[t].begin(), ls[t].end());
     dst.insert(dst.end(), ld[t].begin(), ld[t].end());
+    if (wts) wts->insert(wts->end(), lw[t].begin(), lw[t].end());
   }
   return PLATO_OK;
 }
@@ -191,7 +216,9 @@ int list_files(const std::string& path, std::vector<std::string>* files) {
 
 }  // namespace
 
-extern "C" int plato_edge_list_read_csv(const char* path, plato_edge_list** out) {
+namespace {
+
+int read_csv(const char* path, bool weighted, plato_edge_list** out) {
   if (!path || !out) return set_error(PLATO_EINVAL, "plato_edge_list_read_csv: null argument");
   *out = nullptr;
   try {
@@ -199,10 +226,11 @@ extern "C" int plato_edge_list_read_csv(const char* path, plato_edge_list** out)
     const int lrc = list_files(path, &files);
     if (lrc != PLATO_OK) return lrc;
     auto* el = new plato_edge_list();
+    el->weighted = weighted;
     for (const std::string& f : files) {
       std::string buf;
       int rc = read_whole(f, &buf);
-      if (rc == PLATO_OK) rc = parse_buffer(buf, f, el->src, el->dst);
+      if (rc == PLATO_OK) rc = parse_buffer(buf, f, el->src, el->dst, weighted ? &el->w : nullptr);
       if (rc != PLATO_OK) {
         delete el;
         return rc;
@@ -222,6 +250,22 @@ extern "C" int plato_edge_list_read_csv(const char* path, plato_edge_list** out)
   } catch (const std::bad_alloc&) {
     return set_error(PLATO_ENOMEM, "plato_edge_list_read_csv: host allocation failed");
   }
+}
+
+}  // namespace
+
+extern "C" int plato_edge_list_read_csv(const char* path, plato_edge_list** out) {
+  return read_csv(path, false, out);
+}
+
+extern "C" int plato_edge_list_read_csv_weighted(const char* path, plato_edge_list** out) {
+  return read_csv(path, true, out);
+}
+
+extern "C" int plato_edge_list_weights(const plato_edge_list* el, const double** weights) {
+  if (!el || !weights) return set_error(PLATO_EINVAL, "plato_edge_list_weights: null argument");
+  *weights = el->weighted ? el->w.data() : nullptr;
+  return PLATO_OK;
 }
 
 extern "C" int plato_write_vertex_csv(const char* dir, const char* prefix, const void* values,

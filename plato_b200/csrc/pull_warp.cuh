@@ -48,13 +48,16 @@ struct pull_warp_args {
   float* rcarry;          // [W] partial of the row open at the end of range w
   float* rhead;           // [W] range w's part of its first row when that row began earlier
   double* partials;       // [gridDim.x]
+  const float* w = nullptr;  // per-edge weights (CSC order) of a weighted pull, else unused
 };
 
 __device__ __forceinline__ uint32_t warp_range_begin(uint32_t T, uint32_t w, uint32_t W) {
   return static_cast<uint32_t>(static_cast<uint64_t>(T) * w / W);
 }
 
-template <int IPT, class Update>
+// kWeighted: y(v) = sum over in-edges of x[src] * w[edge] (weighted_pagerank.hpp:112-118
+// with x = rank / out-weight-sum), the weights read alongside the ids.
+template <int IPT, class Update, bool kWeighted = false>
 __global__ void __launch_bounds__(1024, 1) k_pull_warp(pull_warp_args a, Update upd) {
   using C = pull_warp_cfg<IPT>;
   constexpr int ITEMS = C::kItems;
@@ -88,10 +91,12 @@ __global__ void __launch_bounds__(1024, 1) k_pull_warp(pull_warp_args a, Update 
     uint32_t i0 = row0, i1 = a.trow[tb + 1];
     uint64_t j0 = a.tedge[tb], j1 = a.tedge[tb + 1];
     uint32_t ids[IPT];
+    float wts[IPT];
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
       const uint64_t e = j0 + lane + 32 * k;
       ids[k] = e < a.E ? __ldg(a.adj + e) : 0u;
+      if constexpr (kWeighted) wts[k] = e < a.E ? __ldg(a.w + e) : 0.f;
     }
     for (uint32_t t = tb; t < te; ++t) {
       const int nrows = static_cast<int>(i1 - i0);
@@ -102,6 +107,7 @@ __global__ void __launch_bounds__(1024, 1) k_pull_warp(pull_warp_args a, Update 
       for (int k = 0; k < IPT; ++k) {
         const uint32_t s = ids[k];
         vals[k] = (lane + 32 * k < nnz) ? (s < a.H ? s_hub[s] : __ldg(a.x + s)) : 0.f;
+        if constexpr (kWeighted) vals[k] *= wts[k];
       }
       uint32_t re[IPT];
 #pragma unroll
@@ -119,6 +125,7 @@ __global__ void __launch_bounds__(1024, 1) k_pull_warp(pull_warp_args a, Update 
         for (int k = 0; k < IPT; ++k) {
           const uint64_t e = j1 + lane + 32 * k;
           ids[k] = e < a.E ? __ldg(a.adj + e) : 0u;
+          if constexpr (kWeighted) wts[k] = e < a.E ? __ldg(a.w + e) : 0.f;
         }
       }
 #pragma unroll

@@ -25,19 +25,23 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 GRAPHS = ["graph_10_9.csv", "v100_e2150_ua_c3.csv", "v100_e4300_da_c3.csv", "raw_graph_7_7.csv"]
+WEIGHTED_GRAPHS = ["raw_graph_10_9_weighted.csv"]  # `src,dst,w` (double_decoder, parsers.hpp:84-88)
 
 
-def parse_csv(path: Path) -> tuple[np.ndarray, np.ndarray]:
-    src, dst = [], []
+def parse_csv(path: Path, weighted: bool = False):
+    src, dst, w = [], [], []
     for line in path.read_text().splitlines():
         if not line:
             continue
         parts = line.split(",")
-        if len(parts) < 2:
+        if len(parts) < (3 if weighted else 2):
             continue
         src.append(int(parts[0].strip() or 0))
         dst.append(int(parts[1].strip() or 0))
-    return np.asarray(src, dtype=np.uint32), np.asarray(dst, dtype=np.uint32)
+        if weighted:
+            w.append(float(parts[2]))
+    out = (np.asarray(src, dtype=np.uint32), np.asarray(dst, dtype=np.uint32))
+    return out + (np.asarray(w, dtype=np.float64),) if weighted else out
 
 
 KATS = {
@@ -133,6 +137,12 @@ def main(root: Path) -> None:
         key = name.replace(".csv", "")
         arrays[f"{key}__src"] = s
         arrays[f"{key}__dst"] = d
+    for name in WEIGHTED_GRAPHS:
+        s, d, w = parse_csv(root / "data" / "graph" / name, weighted=True)
+        key = name.replace(".csv", "")
+        arrays[f"{key}__src"] = s
+        arrays[f"{key}__dst"] = d
+        arrays[f"{key}__w"] = w
     np.savez_compressed(HERE / "fixtures.npz", **arrays)
     (HERE / "kats.json").write_text(json.dumps(KATS, indent=1) + "\n")
     np.savez_compressed(HERE / "hll_golden.npz", **hll_vectors(root))

@@ -30,6 +30,21 @@ def test_csv_line_rules(tmp_path):
     assert V == 9
 
 
+def test_csv_weighted_line_rules(tmp_path):
+    # double_decoder (parsers.hpp:84-88): the third strtok field through
+    # strtod; a line without one fails to decode and is skipped
+    text = "0,1,2.5\n1,2\n 2 , 3 , 1e2\n,,4,,6,,-0.25,9\n5,6,abc\n7,8, \n7,8,0x10\n9,1,3"
+    _write(tmp_path / "w.csv", text)
+    V, s, d, w = pb.read_csv(tmp_path / "w.csv", weighted=True)
+    assert s.tolist() == [0, 2, 4, 5, 7, 7, 9]
+    assert d.tolist() == [1, 3, 6, 6, 8, 8, 1]
+    assert w.tolist() == [2.5, 100.0, -0.25, 0.0, 0.0, 16.0, 3.0]
+    assert V == 10
+    # the unweighted reader ignores the third field
+    V2, s2, d2 = pb.read_csv(tmp_path / "w.csv")
+    assert s2.size == 8 and V2 == 10
+
+
 def test_csv_last_line_without_newline_and_empty_file(tmp_path):
     _write(tmp_path / "a.csv", "3,4\n4,5")
     V, s, d = pb.read_csv(tmp_path / "a.csv")
