@@ -443,7 +443,6 @@ plato_graph::~plato_graph() {
   plato_b200::destroy_rank_workspace(rank_ws);
   plato_b200::destroy_bfs_workspace(bfs_ws);
   plato_b200::destroy_hll_workspace(hll_ws);
-  plato_b200::destroy_wpr_workspace(wpr_ws);
   if (stream) cudaStreamDestroy(stream);
 }
 

@@ -25,11 +25,9 @@ struct rank_workspace;   // rank.cu
 struct bfs_workspace;    // bfs.cu
 class batch_engine;      // ppr_batch.cu
 struct hll_workspace;    // hll.cu
-struct wpr_workspace;    // wpagerank.cu
 void destroy_rank_workspace(rank_workspace*);
 void destroy_bfs_workspace(bfs_workspace*);
 void destroy_hll_workspace(hll_workspace*);
-void destroy_wpr_workspace(wpr_workspace*);
 void destroy_batch_engine(batch_engine*);
 
 }  // namespace plato_b200
@@ -55,7 +53,6 @@ struct plato_graph {
   plato_b200::rank_workspace* rank_ws = nullptr;
   plato_b200::bfs_workspace* bfs_ws = nullptr;
   plato_b200::hll_workspace* hll_ws = nullptr;  // HyperLogLog buffers (hll.cu)
-  plato_b200::wpr_workspace* wpr_ws = nullptr;  // weighted PageRank buffers (wpagerank.cu)
   plato_b200::batch_engine* batch_cache = nullptr;  // plato_ppr_batch state, kept between calls
   std::vector<uint32_t> h_to_int;             // host copy of to_int (lazily)
   std::map<uint32_t, uint32_t> batch_tuned;   // K bucket -> columns per tile (kt)

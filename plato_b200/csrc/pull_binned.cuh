@@ -21,6 +21,9 @@
 // streamed arrays (ids, offsets, degrees, old ranks) are read with
 // evict-first loads so they do not push those ranks out of L1 and L2.  Every
 // row is summed in a fixed order, so results are bit-for-bit reproducible.
+// With kW (weighted PageRank, weighted_pagerank.hpp:112-118) each gathered
+// value is multiplied by its edge's weight, read like the ids from w (CSC
+// order), pipelined with them.
 #pragma once
 
 #include "common.cuh"
@@ -63,6 +66,17 @@ struct round_ids {
   }
 };
 
+// Weights of one round, at the same positions as round_ids.
+struct round_w {
+  float w0, w1, w2, w3;
+  __device__ __forceinline__ void load(const float* __restrict__ wb, uint32_t j, uint32_t e) {
+    w0 = j < e ? __ldcs(wb + j) : 0.f;
+    w1 = j + 32 < e ? __ldcs(wb + j + 32) : 0.f;
+    w2 = j + 64 < e ? __ldcs(wb + j + 64) : 0.f;
+    w3 = j + 96 < e ? __ldcs(wb + j + 96) : 0.f;
+  }
+};
+
 // One warp per unit.  A unit's segments (one hub piece, or up to 32 whole
 // rows) are walked in rounds of 128 edges, software-pipelined one round
 // deep: the ids of the next round (possibly of the next row) are loaded
@@ -70,11 +84,12 @@ struct round_ids {
 // overlap instead of running back to back.  Lane j keeps the sum of segment
 // j and applies the update of row row0+j, so the offsets, degrees and old
 // ranks of a group are read with one coalesced access each.
-template <class Update>
+template <class Update, bool kW = false>
 __global__ void __launch_bounds__(256, 8) k_pull_long(pull_plan_view pv, const uint64_t* __restrict__ off,
                                                    const uint32_t* __restrict__ adj,
                                                    const float* __restrict__ x, Update upd,
-                                                   double* __restrict__ partials) {
+                                                   double* __restrict__ partials,
+                                                   const float* __restrict__ w) {
   __shared__ double s_red[32];
   if (upd.skip()) return;
   const unsigned lane = threadIdx.x & 31;
@@ -106,10 +121,13 @@ __global__ void __launch_bounds__(256, 8) k_pull_long(pull_plan_view pv, const u
     const bool mine = !piece && lane < nseg;
     const typename Update::operands ops = upd.load(mine ? it.x + lane : it.x);
     const uint32_t* ab = adj + base;
+    const float* wb = kW ? w + base : nullptr;
     uint32_t k = 0;
     uint32_t i = __shfl_sync(0xffffffffu, sb, 0), e = __shfl_sync(0xffffffffu, se, 0);
     round_ids cur;
     cur.load(ab, i + lane, e);
+    round_w cw{0.f, 0.f, 0.f, 0.f};
+    if constexpr (kW) cw.load(wb, i + lane, e);
     float s = 0.f, res = 0.f;
     for (;;) {
       // cursor of the next round (warp-uniform)
@@ -122,12 +140,23 @@ __global__ void __launch_bounds__(256, 8) k_pull_long(pull_plan_view pv, const u
       }
       const bool more = kn < nseg;
       round_ids nxt{0u, 0u, 0u, 0u};
-      if (more) nxt.load(ab, in + lane, en);
+      round_w nw{0.f, 0.f, 0.f, 0.f};
+      if (more) {
+        nxt.load(ab, in + lane, en);
+        if constexpr (kW) nw.load(wb, in + lane, en);
+      }
       const uint32_t j = i + lane;
-      const float g0 = j < e ? __ldg(x + cur.a0) : 0.f;
-      const float g1 = j + 32 < e ? __ldg(x + cur.a1) : 0.f;
-      const float g2 = j + 64 < e ? __ldg(x + cur.a2) : 0.f;
-      const float g3 = j + 96 < e ? __ldg(x + cur.a3) : 0.f;
+      float g0 = j < e ? __ldg(x + cur.a0) : 0.f;
+      float g1 = j + 32 < e ? __ldg(x + cur.a1) : 0.f;
+      float g2 = j + 64 < e ? __ldg(x + cur.a2) : 0.f;
+      float g3 = j + 96 < e ? __ldg(x + cur.a3) : 0.f;
+      if constexpr (kW) {
+        g0 *= cw.w0;
+        g1 *= cw.w1;
+        g2 *= cw.w2;
+        g3 *= cw.w3;
+        cw = nw;
+      }
       s += (g0 + g1) + (g2 + g3);
       if (kn != k) {
         const float t = warp_sum(s);
@@ -185,6 +214,17 @@ struct row_ids {
   }
 };
 
+template <int LPR>
+struct row_w {
+  float w0, w1, w2, w3;
+  __device__ __forceinline__ void load(const float* __restrict__ wb, uint32_t j, uint32_t e) {
+    w0 = j < e ? __ldcs(wb + j) : 0.f;
+    w1 = j + LPR < e ? __ldcs(wb + j + LPR) : 0.f;
+    w2 = j + 2 * LPR < e ? __ldcs(wb + j + 2 * LPR) : 0.f;
+    w3 = j + 3 * LPR < e ? __ldcs(wb + j + 3 * LPR) : 0.f;
+  }
+};
+
 // Rows [r0, r1) whose in-degree is at most 4*LPR.  One warp per unit of 32
 // consecutive rows; a round gives each row LPR lanes with four edges each, so
 // it covers 32/LPR rows and a unit takes LPR rounds.  The ids of the next
@@ -192,11 +232,12 @@ struct row_ids {
 // the warp's next unit and the update operands of this unit are loaded at the
 // start of the unit.  Lane j ends up with the sum of row row0+j, so offsets,
 // operands and new ranks move with one coalesced access each.
-template <int LPR, class Update>
+template <int LPR, class Update, bool kW = false>
 __global__ void __launch_bounds__(256, 8) k_pull_rows(uint32_t r0, uint32_t r1, const uint64_t* __restrict__ off,
                                                    const uint32_t* __restrict__ adj,
                                                    const float* __restrict__ x, Update upd,
-                                                   double* __restrict__ partials) {
+                                                   double* __restrict__ partials,
+                                                   const float* __restrict__ w) {
   static_assert(LPR == 4 || LPR == 8 || LPR == 16, "k_pull_rows: 4, 8 or 16 lanes per row");
   constexpr uint32_t RPR = 32 / LPR;  // rows per round
   __shared__ double s_red[32];
@@ -224,24 +265,36 @@ __global__ void __launch_bounds__(256, 8) k_pull_rows(uint32_t r0, uint32_t r1, 
     const uint32_t sb = mine ? static_cast<uint32_t>(lo - base) : 0u;
     const uint32_t se = mine ? static_cast<uint32_t>(hi - base) : 0u;
     const uint32_t* ab = adj + base;
+    const float* wb = kW ? w + base : nullptr;
     uint32_t b = __shfl_sync(0xffffffffu, sb, slot), e = __shfl_sync(0xffffffffu, se, slot);
     row_ids<LPR> cur;
     cur.load(ab, b + q, e);
+    row_w<LPR> cw{0.f, 0.f, 0.f, 0.f};
+    if constexpr (kW) cw.load(wb, b + q, e);
     float res = 0.f;
 #pragma unroll 1
     for (uint32_t t = 0; t < LPR; ++t) {  // 32 rows / RPR rows per round = LPR rounds
       uint32_t bn = 0, en = 0;
       row_ids<LPR> nxt{0u, 0u, 0u, 0u};
+      row_w<LPR> nw{0.f, 0.f, 0.f, 0.f};
       if (t + 1 < LPR) {
         bn = __shfl_sync(0xffffffffu, sb, (t + 1) * RPR + slot);
         en = __shfl_sync(0xffffffffu, se, (t + 1) * RPR + slot);
         nxt.load(ab, bn + q, en);
+        if constexpr (kW) nw.load(wb, bn + q, en);
       }
       const uint32_t j = b + q;
-      const float g0 = j < e ? __ldg(x + cur.a0) : 0.f;
-      const float g1 = j + LPR < e ? __ldg(x + cur.a1) : 0.f;
-      const float g2 = j + 2 * LPR < e ? __ldg(x + cur.a2) : 0.f;
-      const float g3 = j + 3 * LPR < e ? __ldg(x + cur.a3) : 0.f;
+      float g0 = j < e ? __ldg(x + cur.a0) : 0.f;
+      float g1 = j + LPR < e ? __ldg(x + cur.a1) : 0.f;
+      float g2 = j + 2 * LPR < e ? __ldg(x + cur.a2) : 0.f;
+      float g3 = j + 3 * LPR < e ? __ldg(x + cur.a3) : 0.f;
+      if constexpr (kW) {
+        g0 *= cw.w0;
+        g1 *= cw.w1;
+        g2 *= cw.w2;
+        g3 *= cw.w3;
+        cw = nw;
+      }
       float s = (g0 + g1) + (g2 + g3);
 #pragma unroll
       for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -260,11 +313,12 @@ __global__ void __launch_bounds__(256, 8) k_pull_rows(uint32_t r0, uint32_t r1, 
   if (threadIdx.x == 0) partials[blockIdx.x] = dl;
 }
 
-template <class Update>
+template <class Update, bool kW = false>
 __global__ void __launch_bounds__(256) k_pull_short(pull_plan_view pv, const uint64_t* __restrict__ off,
                                                     const uint32_t* __restrict__ adj,
                                                     const float* __restrict__ x, Update upd,
-                                                    double* __restrict__ partials) {
+                                                    double* __restrict__ partials,
+                                                    const float* __restrict__ w) {
   __shared__ double s_red[32];
   if (upd.skip()) return;
   const uint32_t base = pv.short_begin;
@@ -280,8 +334,14 @@ __global__ void __launch_bounds__(256) k_pull_short(pull_plan_view pv, const uin
     const uint32_t a1 = p1 ? __ldcs(adj + b + 1) : 0u;
     const uint32_t a2 = p2 ? __ldcs(adj + b + 2) : 0u;
     const uint32_t a3 = p3 ? __ldcs(adj + b + 3) : 0u;
-    const float g0 = p0 ? __ldg(x + a0) : 0.f, g1 = p1 ? __ldg(x + a1) : 0.f;
-    const float g2 = p2 ? __ldg(x + a2) : 0.f, g3 = p3 ? __ldg(x + a3) : 0.f;
+    float g0 = p0 ? __ldg(x + a0) : 0.f, g1 = p1 ? __ldg(x + a1) : 0.f;
+    float g2 = p2 ? __ldg(x + a2) : 0.f, g3 = p3 ? __ldg(x + a3) : 0.f;
+    if constexpr (kW) {
+      g0 *= p0 ? __ldcs(w + b) : 0.f;
+      g1 *= p1 ? __ldcs(w + b + 1) : 0.f;
+      g2 *= p2 ? __ldcs(w + b + 2) : 0.f;
+      g3 *= p3 ? __ldcs(w + b + 3) : 0.f;
+    }
     const float s = (g0 + g1) + (g2 + g3);
     dl += upd.apply(v, s);
   }

@@ -38,6 +38,7 @@ struct pull_plan {
 
 struct rank_workspace {
   dbuf<float> x[2];
+  dbuf<float> r[2];  // weighted PageRank: ranks (x holds rank / out-weight sum)
   dbuf<float> y;  // push-mode accumulator
   dbuf<float> carry, head;
   dbuf<double> partials;
@@ -68,20 +69,56 @@ namespace {
 constexpr int kIPT = PLATO_PULL_IPT;  // merge items per lane (odd: spreads lanes over banks)
 using cfg = pull_warp_cfg<kIPT>;
 
+// Update of weighted PageRank (weighted_pagerank.hpp:112-137): the pull
+// gathers x = rank / v_weight_sum times each edge's weight;
+// rank' = 1 - d + d * y, x' = rank' / v_weight_sum, delta += |rank' - rank|.
+// A vertex whose out-weights sum to 0 gets x' = inf, so its edges give
+// inf * 0 = NaN, as the reference's 0 / 0 does.
+struct wrank_update {
+  const float* __restrict__ r;     // current ranks
+  float* __restrict__ rn;          // next ranks
+  float* __restrict__ xn;          // next gathered state
+  const float* __restrict__ wsum;  // v_weight_sum
+  float base;                      // 1 - d
+  float d;
+  int final_epoch;
+
+  __device__ __forceinline__ bool skip() const { return false; }
+
+  struct operands {
+    float ro;
+    float ws;
+  };
+  __device__ __forceinline__ operands load(uint32_t v) const {
+    if (final_epoch) return {0.f, 1.f};
+    return {__ldcs(r + v), __ldcs(wsum + v)};
+  }
+
+  __device__ __forceinline__ double apply(uint32_t v, float y) const { return apply(v, y, load(v)); }
+
+  __device__ __forceinline__ double apply(uint32_t v, float y, operands o) const {
+    const float rv = fmaf(d, y, base);
+    rn[v] = rv;
+    if (final_epoch) return 0.0;
+    xn[v] = rv / o.ws;
+    return static_cast<double>(fabsf(rv - o.ro));
+  }
+};
+
 // Opts the kernel into the largest dynamic shared memory the device allows
 // next to its static shared memory; returns the hub capacity (floats) that fits.
-template <class Tele>
+template <class Upd, bool kW = false>
 int set_pull_smem_attr(int device, uint32_t* hub_cap) {
   static uint32_t cap = 0;
   if (cap == 0) {
     int optin = 0;
     PLATO_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
     cudaFuncAttributes fa{};
-    PLATO_CUDA_TRY(cudaFuncGetAttributes(&fa, k_pull_warp<kIPT, rank_update<Tele>>));
+    PLATO_CUDA_TRY(cudaFuncGetAttributes(&fa, k_pull_warp<kIPT, Upd, kW>));
     const size_t dyn = static_cast<size_t>(optin) - fa.sharedSizeBytes;
     if (dyn <= cfg::kSlices + 64)
       return set_error(PLATO_ECUDA, "pull kernel: not enough shared memory on this device");
-    PLATO_CUDA_TRY(cudaFuncSetAttribute(k_pull_warp<kIPT, rank_update<Tele>>,
+    PLATO_CUDA_TRY(cudaFuncSetAttribute(k_pull_warp<kIPT, Upd, kW>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(dyn)));
     cap = static_cast<uint32_t>((dyn - cfg::kSlices - 16) / 4 / 32 * 32);
@@ -198,11 +235,12 @@ int ensure_ws(plato_graph* g, cudaStream_t st) {
   if (!ws->h_delta) PLATO_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&ws->h_delta), sizeof(double)));
   if (!ws->h_ctrl) PLATO_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&ws->h_ctrl), 2 * sizeof(int)));
   uint32_t cap_a = 0, cap_b = 0;
-  PLATO_TRY(set_pull_smem_attr<teleport_uniform>(g->device, &cap_a));
-  PLATO_TRY(set_pull_smem_attr<teleport_single>(g->device, &cap_b));
-  uint32_t cap_c = 0;
-  PLATO_TRY(set_pull_smem_attr<teleport_seeds>(g->device, &cap_c));
-  cap_b = std::min(cap_b, cap_c);
+  PLATO_TRY(set_pull_smem_attr<rank_update<teleport_uniform>>(g->device, &cap_a));
+  PLATO_TRY(set_pull_smem_attr<rank_update<teleport_single>>(g->device, &cap_b));
+  uint32_t cap_c = 0, cap_d = 0;
+  PLATO_TRY(set_pull_smem_attr<rank_update<teleport_seeds>>(g->device, &cap_c));
+  PLATO_TRY((set_pull_smem_attr<wrank_update, true>(g->device, &cap_d)));
+  cap_b = std::min(cap_b, std::min(cap_c, cap_d));
   ws->hub_cap = std::min(cap_a, cap_b);
   return PLATO_OK;
 }
@@ -229,13 +267,13 @@ __global__ void k_init_single(const uint32_t* __restrict__ deg, uint32_t V, uint
   }
 }
 
-// One pull epoch: persistent warp-tile gather + cross-range fixup; partial
-// deltas to ws->partials (one per CTA, then one per fixup block).
-template <class Tele>
-int pull_epoch(plato_graph* g, const float* x, float* xn, Tele tele, float d, bool final_epoch,
-               cudaStream_t st, const int* mode = nullptr) {
+// One pull epoch gathering x (times the edge weights w when kW) with the
+// fused update `upd`: the degree bins on a relabelled graph, else the
+// persistent warp-tile merge path + cross-range fixup.  Partial deltas go to
+// ws->partials (one per CTA of each kernel).
+template <class Upd, bool kW>
+int pull_epoch_with(plato_graph* g, const float* x, const Upd& upd, const float* w, cudaStream_t st) {
   rank_workspace* ws = g->rank_ws;
-  rank_update<Tele> upd{x, xn, g->out_deg.p, tele, d, final_epoch ? 1 : 0, mode};
   const pull_plan& pl = ws->plan;
   if (pl.valid) {
     const pull_plan_view pv{pl.n_long, pl.rows_begin[3], g->info.vertices, pl.n_items, pl.items.p,
@@ -244,40 +282,40 @@ int pull_epoch(plato_graph* g, const float* x, float* xn, Tele tele, float d, bo
     double* part = ws->partials.p;
     if (pl.blocks_long) {
       prof_scope ps("k_pull_long", st);
-      k_pull_long<rank_update<Tele>><<<pl.blocks_long, 256, 0, st>>>(pv, g->in_off.p, g->in_adj.p, x, upd, part);
+      k_pull_long<Upd, kW><<<pl.blocks_long, 256, 0, st>>>(pv, g->in_off.p, g->in_adj.p, x, upd, part, w);
       PLATO_LAUNCHED("k_pull_long");
     }
     part += pl.blocks_long;
     if (pl.blocks_hubs) {
       prof_scope ps("k_pull_hubs", st);
-      k_pull_hubs<rank_update<Tele>><<<pl.blocks_hubs, 256, 0, st>>>(pv, upd, part);
+      k_pull_hubs<Upd><<<pl.blocks_hubs, 256, 0, st>>>(pv, upd, part);
       PLATO_LAUNCHED("k_pull_hubs");
     }
     part += pl.blocks_hubs;
     if (pl.blocks_rows[0]) {
       prof_scope ps("k_pull_rows16", st);
-      k_pull_rows<16, rank_update<Tele>><<<pl.blocks_rows[0], 256, 0, st>>>(
-          pl.rows_begin[0], pl.rows_begin[1], g->in_off.p, g->in_adj.p, x, upd, part);
+      k_pull_rows<16, Upd, kW><<<pl.blocks_rows[0], 256, 0, st>>>(
+          pl.rows_begin[0], pl.rows_begin[1], g->in_off.p, g->in_adj.p, x, upd, part, w);
       PLATO_LAUNCHED("k_pull_rows16");
     }
     part += pl.blocks_rows[0];
     if (pl.blocks_rows[1]) {
       prof_scope ps("k_pull_rows8", st);
-      k_pull_rows<8, rank_update<Tele>><<<pl.blocks_rows[1], 256, 0, st>>>(
-          pl.rows_begin[1], pl.rows_begin[2], g->in_off.p, g->in_adj.p, x, upd, part);
+      k_pull_rows<8, Upd, kW><<<pl.blocks_rows[1], 256, 0, st>>>(
+          pl.rows_begin[1], pl.rows_begin[2], g->in_off.p, g->in_adj.p, x, upd, part, w);
       PLATO_LAUNCHED("k_pull_rows8");
     }
     part += pl.blocks_rows[1];
     if (pl.blocks_rows[2]) {
       prof_scope ps("k_pull_rows4", st);
-      k_pull_rows<4, rank_update<Tele>><<<pl.blocks_rows[2], 256, 0, st>>>(
-          pl.rows_begin[2], pl.rows_begin[3], g->in_off.p, g->in_adj.p, x, upd, part);
+      k_pull_rows<4, Upd, kW><<<pl.blocks_rows[2], 256, 0, st>>>(
+          pl.rows_begin[2], pl.rows_begin[3], g->in_off.p, g->in_adj.p, x, upd, part, w);
       PLATO_LAUNCHED("k_pull_rows4");
     }
     part += pl.blocks_rows[2];
     if (pl.blocks_short) {
       prof_scope ps("k_pull_short", st);
-      k_pull_short<rank_update<Tele>><<<pl.blocks_short, 256, 0, st>>>(pv, g->in_off.p, g->in_adj.p, x, upd, part);
+      k_pull_short<Upd, kW><<<pl.blocks_short, 256, 0, st>>>(pv, g->in_off.p, g->in_adj.p, x, upd, part, w);
       PLATO_LAUNCHED("k_pull_short");
     }
     return PLATO_OK;
@@ -285,20 +323,27 @@ int pull_epoch(plato_graph* g, const float* x, float* xn, Tele tele, float d, bo
   const merge_tiles& mt = g->tiles.at(cfg::kItems);
   const uint32_t H = std::min<uint32_t>(g->info.vertices, ws->hub_cap);
   pull_warp_args a{mt.row.p, mt.edge.p, mt.count, g->stored_edges, g->in_off.p, g->in_adj.p,
-                   x, H, ws->carry.p, ws->head.p, ws->partials.p};
+                   x, H, ws->carry.p, ws->head.p, ws->partials.p, w};
   {
     prof_scope ps("k_pull_warp", st);
-    k_pull_warp<kIPT, rank_update<Tele>><<<ws->sms, 1024, cfg::smem_bytes(H), st>>>(a, upd);
+    k_pull_warp<kIPT, Upd, kW><<<ws->sms, 1024, cfg::smem_bytes(H), st>>>(a, upd);
     PLATO_LAUNCHED("k_pull_warp");
   }
   const uint32_t W = ws->sms * cfg::kWarps;
   a.partials = ws->partials.p + ws->sms;
   {
     prof_scope ps("k_pull_warp_fixup", st);
-    k_pull_warp_fixup<rank_update<Tele>><<<(W + 255) / 256, 256, 0, st>>>(a, W, upd);
+    k_pull_warp_fixup<Upd><<<(W + 255) / 256, 256, 0, st>>>(a, W, upd);
     PLATO_LAUNCHED("k_pull_warp_fixup");
   }
   return PLATO_OK;
+}
+
+template <class Tele>
+int pull_epoch(plato_graph* g, const float* x, float* xn, Tele tele, float d, bool final_epoch,
+               cudaStream_t st, const int* mode = nullptr) {
+  const rank_update<Tele> upd{x, xn, g->out_deg.p, tele, d, final_epoch ? 1 : 0, mode};
+  return pull_epoch_with<rank_update<Tele>, false>(g, x, upd, nullptr, st);
 }
 
 int partial_count(const plato_graph* g) {
@@ -550,6 +595,60 @@ int seedset_impl(plato_graph* g, const uint32_t* seeds_ext, uint32_t n, const pl
   return PLATO_OK;
 }
 
+// weighted_pagerank.hpp:104-109: ranks 1, gathered state 1 / v_weight_sum.
+__global__ void k_init_weighted(const float* __restrict__ wsum, uint32_t V, float* r, float* x) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    r[v] = 1.0f;
+    x[v] = 1.0f / wsum[v];
+  }
+}
+
+// algo::weighted_pagerank (weighted_pagerank.hpp:60-149) into d_out (caller
+// ids, the reference's units).  Epochs are the pull epochs of PageRank with
+// the edge weights multiplied into the gathers; with eps > 0 the delta is read
+// back after each non-final epoch and a small one jumps to the last epoch
+// (:131-137).
+int wpagerank_impl(plato_graph* g, const plato_pagerank_opts* o, float* d_out, cudaStream_t st,
+                   plato_run_stats* stats) {
+  if (!g->weighted)
+    return set_error(PLATO_EINVAL, "plato_weighted_pagerank: the graph has no edge weights "
+                                   "(create it with plato_graph_create_weighted)");
+  if (!(o->damping >= 0.0 && o->damping <= 1.0)) return set_error(PLATO_EINVAL, "damping must be in [0, 1]");
+  rank_workspace* ws = g->rank_ws;
+  const uint32_t V = g->info.vertices;
+  PLATO_TRY(ws->r[0].alloc(V));
+  PLATO_TRY(ws->r[1].alloc(V));
+  k_init_weighted<<<grid_for(V, 256), 256, 0, st>>>(g->out_wsum.p, V, ws->r[0].p, ws->x[0].p);
+  PLATO_LAUNCHED("k_init_weighted");
+  const float base = static_cast<float>(1.0 - o->damping), d = static_cast<float>(o->damping);
+  const uint32_t nparts = static_cast<uint32_t>(partial_count(g));
+  int cur = 0;
+  uint32_t epochs = 0;
+  double delta = 0.0;
+  for (uint32_t epoch = 0; epoch < o->iteration; ++epoch) {
+    const bool last = epoch + 1 == o->iteration;
+    const wrank_update upd{ws->r[cur].p, ws->r[cur ^ 1].p, ws->x[cur ^ 1].p, g->out_wsum.p, base, d,
+                           last ? 1 : 0};
+    PLATO_TRY((pull_epoch_with<wrank_update, true>(g, ws->x[cur].p, upd, g->in_w.p, st)));
+    cur ^= 1;
+    ++epochs;
+    if (last) break;
+    if (o->eps > 0.0) {
+      PLATO_TRY(read_delta(g, nparts, st, &delta));
+      if (delta < o->eps) epoch = o->iteration - 2;  // the next epoch is the last
+    }
+  }
+  PLATO_TRY(scatter_to_external_f32(g, ws->r[cur].p, d_out, st));
+  if (stats) {
+    *stats = plato_run_stats{};
+    stats->iterations = epochs;
+    stats->pull_iterations = epochs;
+    stats->delta = delta;
+  }
+  return PLATO_OK;
+}
+
 // Host-buffer wrapper: run into a device staging buffer, copy to `host`.
 template <class F>
 int with_host_output(plato_graph* g, float* host, F&& run) {
@@ -605,5 +704,15 @@ extern "C" int plato_seedset_ppr(plato_graph* g, const plato_vid_t* seeds, uint3
   PLATO_CUDA_TRY(cudaSetDevice(g->device));
   return with_host_output(g, ranks, [&](float* d_out, cudaStream_t st) {
     return seedset_impl(g, seeds, n, opts, d_out, st, stats);
+  });
+}
+
+extern "C" int plato_weighted_pagerank(plato_graph* g, const plato_pagerank_opts* opts, float* ranks,
+                                       plato_run_stats* stats) {
+  if (!g || !opts || !ranks) return set_error(PLATO_EINVAL, "plato_weighted_pagerank: null argument");
+  std::lock_guard<std::mutex> lock(g->mu);
+  PLATO_CUDA_TRY(cudaSetDevice(g->device));
+  return with_host_output(g, ranks, [&](float* d_out, cudaStream_t st) {
+    return wpagerank_impl(g, opts, d_out, st, stats);
   });
 }
