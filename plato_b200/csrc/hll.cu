@@ -184,12 +184,11 @@ struct gather_args {
   double alpha_mm;
 };
 
-// Source rows in flight per lane (VEC 16-byte words each).
-#ifndef PLATO_HLL_ROWS_IN_FLIGHT
-#define PLATO_HLL_ROWS_IN_FLIGHT 8
-#endif
+// Source rows in flight per lane: 8 / VEC (VEC 16-byte words each), at least
+// one (measured on B200: 16 rows lost occupancy to registers at every width).
+constexpr int kRowsInFlight = 8;
 __host__ __device__ constexpr int unroll_for(int vec) {
-  return PLATO_HLL_ROWS_IN_FLIGHT / vec < 1 ? 1 : PLATO_HLL_ROWS_IN_FLIGHT / vec;
+  return kRowsInFlight / vec < 1 ? 1 : kRowsInFlight / vec;
 }
 
 // Source ids a team stages per round (in shared memory, after the filter).
