@@ -264,7 +264,17 @@ __device__ __forceinline__ void bfs_pull_step(const bfs_level_args& a, append_sm
         }
       }
     }
-    if (found) bfs_visit(a, v, par);
+    if (found) {
+      a.level[v] = a.new_level;
+      a.parent[v] = par;
+    }
+    // A warp's rows of a round are 32 consecutive ids on one bitmap word that
+    // no other thread touches during a pull step: one plain update per warp.
+    const unsigned fm = __ballot_sync(0xffffffffu, found);
+    if (lane == 0 && fm) {
+      a.visited[v >> 5] |= fm;
+      a.next.bits[v >> 5] |= fm;
+    }
     frontier_append_block(a.next, found, v, a.out_deg, app);  // block-uniform: same rounds everywhere
   }
 }
