@@ -43,6 +43,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cub/device/device_scan.cuh>
+
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -227,10 +229,10 @@ static __global__ void __launch_bounds__(256) k_compact(const uint32_t* bits, ui
 }
 
 // Pull chunk list: (vertex, first edge) for every kPullChunk edges of every column.
-static __global__ void k_count_chunks(const uint64_t* off, uint32_t V, uint32_t* cnt) {
+static __global__ void k_count_chunks(const uint64_t* off, uint32_t V, uint64_t* cnt) {
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
        v += (uint64_t)gridDim.x * blockDim.x)
-    cnt[v] = static_cast<uint32_t>((off[v + 1] - off[v] + kPullChunk - 1) / kPullChunk);
+    cnt[v] = (off[v + 1] - off[v] + kPullChunk - 1) / kPullChunk;
 }
 
 static __global__ void k_fill_chunks(const uint64_t* off, uint32_t V, const uint64_t* cstart,
@@ -413,24 +415,33 @@ class dualmode_engine_t {
     return static_cast<unsigned>(b);
   }
 
+  // The chunk list of the pull direction, built on the device (counts, a
+  // scan for the start of each column's chunks, then the fill).
   void ensure_chunks() {
     if (chunks_ && chunks_reversed_ == reversed_) return;
     if (chunks_) cudaFree(chunks_);
+    chunks_ = nullptr;
     const uint32_t V = view_.vertices;
-    uint32_t* cnt = nullptr;
+    uint64_t* cnt = nullptr;
     uint64_t* start = nullptr;
-    check_cuda(cudaMalloc(&cnt, 4ull * V), "chunks");
+    void* tmp = nullptr;
+    size_t tmp_bytes = 0;
+    check_cuda(cudaMalloc(&cnt, 8ull * (V ? V : 1)), "chunks");
     check_cuda(cudaMalloc(&start, 8ull * (V + 1)), "chunks");
     detail::k_count_chunks<<<grid(V), 256>>>(in_off(), V, cnt);
-    std::vector<uint32_t> h(V);
-    check_cuda(cudaMemcpy(h.data(), cnt, 4ull * V, cudaMemcpyDeviceToHost), "chunks");
-    std::vector<uint64_t> hs(V + 1, 0);
-    for (uint32_t v = 0; v < V; ++v) hs[v + 1] = hs[v] + h[v];
-    nchunks_ = hs[V];
-    check_cuda(cudaMemcpy(start, hs.data(), 8ull * (V + 1), cudaMemcpyHostToDevice), "chunks");
+    check_cuda(cudaMemset(start, 0, sizeof(uint64_t)), "chunks");
+    check_cuda(cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, cnt, start + 1, static_cast<int64_t>(V)),
+               "chunks");
+    check_cuda(cudaMalloc(&tmp, tmp_bytes ? tmp_bytes : 1), "chunks");
+    check_cuda(cub::DeviceScan::InclusiveSum(tmp, tmp_bytes, cnt, start + 1, static_cast<int64_t>(V)),
+               "chunks");
+    uint64_t total = 0;
+    check_cuda(cudaMemcpy(&total, start + V, sizeof(total), cudaMemcpyDeviceToHost), "chunks");
+    nchunks_ = total;
     check_cuda(cudaMalloc(&chunks_, sizeof(uint2) * (nchunks_ ? nchunks_ : 1)), "chunks");
     detail::k_fill_chunks<<<grid(V), 256>>>(in_off(), V, start, chunks_);
     check_cuda(cudaDeviceSynchronize(), "chunks");
+    cudaFree(tmp);
     cudaFree(cnt);
     cudaFree(start);
     chunks_reversed_ = reversed_;
