@@ -40,6 +40,7 @@ struct bfs_workspace {
   dbuf<uint32_t> level, parent;
   dbuf<bfs_control> ctrl;
   bfs_control* h_ctrl = nullptr;  // pinned
+  unsigned level_blocks = 0;      // one full wave of resident k_bfs_level CTAs
   ~bfs_workspace() {
     if (h_ctrl) cudaFreeHost(h_ctrl);
   }
@@ -349,6 +350,15 @@ __global__ void k_parents_to_external(const uint32_t* __restrict__ parent_int,
   }
 }
 
+// Control word of the first level (bfs.hpp:86-96): push iff the root's
+// out-degree over the stored edges is below the threshold (dualmode.hpp:261-279),
+// decided on the device from the seeded frontier's degree sum.
+__global__ void k_bfs_start(bfs_control* c, const unsigned long long* counters, double edges,
+                            double threshold) {
+  const bool push = (static_cast<double>(counters[2]) / edges) < threshold;
+  *c = bfs_control{push ? 1 : 0, 0, 0, 0, 1ull, push ? 1ull : 0ull, 0u};
+}
+
 int bfs_impl(plato_graph* g, const plato_bfs_opts* o, const plato_dualmode_opts* eo,
              cudaStream_t st, plato_run_stats* stats) {
   const uint32_t V = g->info.vertices;
@@ -356,8 +366,9 @@ int bfs_impl(plato_graph* g, const plato_bfs_opts* o, const plato_dualmode_opts*
   const double threshold = eo ? eo->push_threshold : 0.05;
   PLATO_TRY(ensure_bfs_ws(g));
   bfs_workspace* ws = g->bfs_ws;
-  uint32_t root = 0;
-  PLATO_TRY(lookup_internal(g, o->root, &root, st));
+  const std::vector<uint32_t>* to_int = nullptr;  // host copy, fetched once per graph
+  PLATO_TRY(host_to_internal(g, &to_int, st));
+  const uint32_t root = to_int ? (*to_int)[o->root] : o->root;
   const uint32_t invalid_parent = g->info.max_v_i + 1;  // bfs.hpp:79
   k_bfs_init<<<grid_for(V, 256), 256, 0, st>>>(V, root, invalid_parent, ws->level.p, ws->parent.p,
                                                 ws->visited.p);
@@ -365,20 +376,21 @@ int bfs_impl(plato_graph* g, const plato_bfs_opts* o, const plato_dualmode_opts*
   PLATO_TRY(frontier_reset(ws->fr[0], V, st));
   PLATO_TRY(frontier_reset(ws->fr[1], V, st));
   PLATO_TRY(frontier_seed(ws->fr[0], g, root, st));
-  PLATO_TRY(frontier_read(ws->fr[0], st));
 
   // Level loop with the engine switch on the device (k_bfs_level).  The host
   // enqueues levels in batches and polls between batches; levels enqueued
-  // after the end return at once.
+  // after the end return at once.  Nothing is read back before the first
+  // poll: the first level's mode is set on the device too.
   const double edges = static_cast<double>(g->stored_edges);
-  const bool first_push = (static_cast<double>(ws->fr[0].h_counters[2]) / edges) < threshold;
-  const bfs_control init{first_push ? 1 : 0, 0, 0, 0, 1ull, first_push ? 1ull : 0ull, 0u};
-  PLATO_CUDA_TRY(cudaMemcpyAsync(ws->ctrl.p, &init, sizeof(init), cudaMemcpyHostToDevice, st));
-  // one full wave of resident CTAs; the steps stride over their work
-  int sms = 0, per_sm = 0;
-  PLATO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
-  PLATO_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bfs_level, 256, 0));
-  const unsigned blocks = static_cast<unsigned>(sms) * static_cast<unsigned>(std::max(per_sm, 1));
+  k_bfs_start<<<1, 1, 0, st>>>(ws->ctrl.p, ws->fr[0].counters.p, edges, threshold);
+  PLATO_LAUNCHED("k_bfs_start");
+  if (ws->level_blocks == 0) {  // one full wave of resident CTAs; the steps stride over their work
+    int sms = 0, per_sm = 0;
+    PLATO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
+    PLATO_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bfs_level, 256, 0));
+    ws->level_blocks = static_cast<unsigned>(sms) * static_cast<unsigned>(std::max(per_sm, 1));
+  }
+  const unsigned blocks = ws->level_blocks;
   bfs_level_args a{};
   a.V = V;
   a.out_off = g->out_off.p;
