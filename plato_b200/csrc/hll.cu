@@ -520,6 +520,54 @@ __global__ void __launch_bounds__(kHllThreads) k_hll_spread(
   }
 }
 
+// One push-mode spread epoch (nstepdegrees.hpp:217-229): the active sources
+// scatter over their forward out-edges and mark every destination not yet
+// covered in `next`; a warp walks one active source's edges 32 at a time,
+// sources found by scanning the active bitmap.  `covered` is only read here
+// (the reference merges the epoch's actives into it afterwards, k_bits_or),
+// and a destination counts once, when its bit goes from 0 to 1.
+__global__ void __launch_bounds__(kHllThreads) k_hll_spread_push(
+    const uint64_t* __restrict__ out_off, const uint32_t* __restrict__ out_adj,
+    const uint32_t* __restrict__ active, const uint32_t* __restrict__ covered, uint32_t* next,
+    const uint32_t* __restrict__ fwd_outdeg, uint32_t words, unsigned long long* counters) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t w0 = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
+  const uint64_t nw = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+  unsigned long long n = 0, deg = 0;
+  for (uint64_t w = w0; w < words; w += nw) {
+    uint32_t bits = __ldg(active + w);  // warp-uniform
+    while (bits) {
+      const uint32_t u = static_cast<uint32_t>(w * 32 + (__ffs(bits) - 1));
+      bits &= bits - 1u;
+      const uint64_t b = __ldg(out_off + u), e = __ldg(out_off + u + 1);
+      for (uint64_t c = b + lane; c < e; c += 32) {
+        const uint32_t dst = __ldg(out_adj + c);
+        const uint32_t bit = 1u << (dst & 31);
+        if (!(__ldg(covered + (dst >> 5)) & bit)) {
+          const uint32_t old = atomicOr(next + (dst >> 5), bit);
+          if (!(old & bit)) {
+            ++n;
+            deg += __ldg(fwd_outdeg + dst);
+          }
+        }
+      }
+    }
+  }
+  n = warp_sum(n);
+  deg = warp_sum(deg);
+  if (lane == 0 && n) {
+    atomicAdd(counters, n);
+    atomicAdd(counters + 1, deg);
+  }
+}
+
+// a |= b over `words` bitmap words.
+__global__ void k_bits_or(uint32_t* a, const uint32_t* __restrict__ b, uint32_t words) {
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < words;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+    a[i] |= b[i];
+}
+
 // Count and forward out-degree sum of a vertex set (the switch's weight).
 __global__ void k_bits_weight(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ fwd_outdeg,
                               uint32_t V, unsigned long long* counters) {
@@ -766,6 +814,26 @@ class hll_engine {
     return read_counters(n, deg);
   }
 
+  // One push-mode spread epoch: the actives scatter over their forward
+  // out-edges, then covered |= next.
+  int spread_push(const uint32_t* active, uint32_t* covered, uint32_t* next, unsigned long long* n,
+                  unsigned long long* deg) {
+    PLATO_TRY(clear_bits(next));
+    PLATO_TRY(zero_counters());
+    if (V_) {
+      {
+        prof_scope ps("k_hll_spread_push", st_);
+        k_hll_spread_push<<<grid_for(static_cast<uint64_t>(words_) * 32, kHllThreads, 148u * 16u), kHllThreads,
+                            0, st_>>>(g_->out_off.p, g_->out_adj.p, active, covered, next, g_->out_deg.p,
+                                      words_, ctr_.p);
+        PLATO_LAUNCHED("k_hll_spread_push");
+      }
+      k_bits_or<<<grid_for(words_, kHllThreads), kHllThreads, 0, st_>>>(covered, next, words_);
+      PLATO_LAUNCHED("k_bits_or");
+    }
+    return read_counters(n, deg);
+  }
+
   int sum_estimates(double* out) {
     if (!V_) {
       *out = 0.0;
@@ -1005,9 +1073,11 @@ int nstep_impl(plato_graph* g, const plato_nstep_opts* o, const plato_dualmode_o
     for (uint32_t i = 0; i < steps && actives > 0; ++i) {
       const bool push = is_push(ae, E, thr);
       record_mode(st, push);
-      // push scatters forward; a reversed pull tests out-neighbours
-      const hll_direction& d = (push || !spread_reversed) ? fwd : rev;
-      PLATO_TRY(h.spread(d, act, covered, nxt, &actives, &ae));
+      if (push) {  // the actives scatter forward (also when the phase is reversed)
+        PLATO_TRY(h.spread_push(act, covered, nxt, &actives, &ae));
+      } else {     // a pull tests in-neighbours, or out-neighbours when reversed
+        PLATO_TRY(h.spread(spread_reversed ? rev : fwd, act, covered, nxt, &actives, &ae));
+      }
       std::swap(act, nxt);
     }
     const bool prop_reversed = !counting_in;
