@@ -568,6 +568,126 @@ __global__ void k_bits_or(uint32_t* a, const uint32_t* __restrict__ b, uint32_t 
     a[i] |= b[i];
 }
 
+// Push-mode propagation epoch (hyperanf.hpp:133-147, nstepdegrees.hpp:316-327):
+// the rows of the active sources scatter over their forward out-edges into
+// nxt with a per-byte max, in three launches.
+//   k_hll_sync_rows  nxt = cur for the stale rows (those that changed last
+//                    epoch), so every row a source may raise starts equal in
+//                    both buffers;
+//   k_hll_scatter    a warp per active source, 32 register words a step:
+//                    rows of at most 32 words serve 32 / W destinations at
+//                    once; a word is raised with compare-and-swap (register
+//                    values only grow, so a stale read never skips a raise);
+//                    a destination whose row rose gets its changed bit;
+//   k_hll_finish     estimate, count and forward out-degree of each changed
+//                    row.
+// Rows outside `covered` (when given) are never written.
+__device__ __forceinline__ uint32_t bitmap_word(const uint32_t* bits, uint64_t w, uint32_t V) {
+  if (bits) return __ldg(bits + w);
+  const uint64_t lo = w * 32;
+  return V - lo >= 32 ? 0xFFFFFFFFu : ((1u << (V - lo)) - 1u);
+}
+
+__global__ void __launch_bounds__(kHllThreads) k_hll_sync_rows(const uint32_t* __restrict__ stale, uint32_t words,
+                                                              const uint8_t* __restrict__ cur, uint8_t* nxt,
+                                                              uint32_t m) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t w0 = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
+  const uint64_t nw = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+  const uint32_t q = m / 16;
+  for (uint64_t w = w0; w < words; w += nw) {
+    uint32_t bits = __ldg(stale + w);
+    while (bits) {
+      const uint64_t v = w * 32 + (__ffs(bits) - 1);
+      bits &= bits - 1u;
+      const uint4* src = reinterpret_cast<const uint4*>(cur + v * m);
+      uint4* dst = reinterpret_cast<uint4*>(nxt + v * m);
+      for (uint32_t i = lane; i < q; i += 32) dst[i] = __ldg(src + i);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kHllThreads) k_hll_scatter(
+    const uint32_t* __restrict__ active, uint32_t V, const uint64_t* __restrict__ out_off,
+    const uint32_t* __restrict__ out_adj, const uint32_t* __restrict__ covered,
+    const uint32_t* __restrict__ cur, uint32_t* nxt, uint32_t* changed, uint32_t m) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t w0 = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
+  const uint64_t nw = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+  const uint32_t W = m / 4;                       // register words per row
+  const uint32_t Wc = W < 32 ? W : 32;            // words per destination and step
+  const uint32_t G = 32 / Wc;                     // destinations per step
+  const uint32_t slot = lane / Wc, wi = lane % Wc;
+  const bool lane_on = slot < G;
+  const uint32_t passes = W / Wc;
+  const uint64_t words = (static_cast<uint64_t>(V) + 31) / 32;
+  for (uint64_t w = w0; w < words; w += nw) {
+    uint32_t bits = bitmap_word(active, w, V);  // warp-uniform
+    while (bits) {
+      const uint32_t u = static_cast<uint32_t>(w * 32 + (__ffs(bits) - 1));
+      bits &= bits - 1u;
+      const uint64_t b = __ldg(out_off + u), e = __ldg(out_off + u + 1);
+      for (uint32_t pass = 0; pass < passes; ++pass) {
+        const uint32_t col = pass * Wc + wi;
+        const uint32_t mine = lane_on ? __ldg(cur + static_cast<size_t>(u) * W + col) : 0u;
+        for (uint64_t c = b + slot; c < e; c += G) {
+          if (!lane_on) break;
+          const uint32_t v = __ldg(out_adj + c);
+          if (covered && !test_bit(covered, v)) continue;
+          uint32_t* p = nxt + static_cast<size_t>(v) * W + col;
+          uint32_t old = *p;
+          for (;;) {  // ends: every failed swap saw a word that grew, and words only grow
+            const uint32_t want = bmax(old, mine);
+            if (want == old) break;
+            const uint32_t prev = atomicCAS(p, old, want);
+            if (prev == old) {
+              atomicOr(changed + (v >> 5), 1u << (v & 31));
+              break;
+            }
+            old = prev;
+          }
+        }
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kHllThreads) k_hll_finish(
+    const uint32_t* __restrict__ changed, uint32_t words, const uint8_t* __restrict__ nxt, double* est,
+    uint32_t P, uint32_t m, double alpha_mm, const uint32_t* __restrict__ fwd_outdeg,
+    unsigned long long* counters) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t w0 = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
+  const uint64_t nw = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+  const uint32_t q = m / 16;
+  unsigned long long n = 0, deg = 0;
+  for (uint64_t w = w0; w < words; w += nw) {
+    uint32_t bits = __ldg(changed + w);
+    while (bits) {
+      const uint64_t v = w * 32 + (__ffs(bits) - 1);
+      bits &= bits - 1u;
+      const uint4* row = reinterpret_cast<const uint4*>(nxt + v * m);
+      unsigned long long sfx = 0;
+      uint32_t zeros = 0;
+      for (uint32_t i = lane; i < q; i += 32) acc_regs(row[i], sfx, zeros);
+      sfx = warp_sum(sfx);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) zeros += __shfl_xor_sync(0xFFFFFFFFu, zeros, o);
+      if (lane == 0) {
+        est[v] = hll_estimate(P, alpha_mm, sfx, zeros);
+        ++n;
+        deg += __ldg(fwd_outdeg + v);
+      }
+    }
+  }
+  n = warp_sum(n);
+  deg = warp_sum(deg);
+  if (lane == 0 && n) {
+    atomicAdd(counters, n);
+    atomicAdd(counters + 1, deg);
+  }
+}
+
 // Count and forward out-degree sum of a vertex set (the switch's weight).
 __global__ void k_bits_weight(const uint32_t* __restrict__ bits, const uint32_t* __restrict__ fwd_outdeg,
                               uint32_t V, unsigned long long* counters) {
@@ -800,6 +920,33 @@ class hll_engine {
     return read_counters(n_changed, deg_changed);
   }
 
+  // One push-mode propagation epoch: the rows of `active` (every vertex when
+  // null) scatter over their forward out-edges.  Counters as for epoch().
+  int epoch_push(const uint32_t* active, const uint32_t* covered, const uint32_t* stale, uint32_t* changed,
+                 unsigned long long* n_changed, unsigned long long* deg_changed) {
+    PLATO_TRY(clear_bits(changed));
+    PLATO_TRY(zero_counters());
+    if (V_) {
+      const unsigned grid = grid_for(static_cast<uint64_t>(words_) * 32, kHllThreads, 148u * 16u);
+      if (stale) {
+        k_hll_sync_rows<<<grid, kHllThreads, 0, st_>>>(stale, words_, cur_, nxt_, m_);
+        PLATO_LAUNCHED("k_hll_sync_rows");
+      }
+      {
+        prof_scope ps("k_hll_scatter", st_);
+        k_hll_scatter<<<grid, kHllThreads, 0, st_>>>(active, V_, g_->out_off.p, g_->out_adj.p, covered,
+                                                     reinterpret_cast<const uint32_t*>(cur_),
+                                                     reinterpret_cast<uint32_t*>(nxt_), changed, m_);
+        PLATO_LAUNCHED("k_hll_scatter");
+      }
+      k_hll_finish<<<grid, kHllThreads, 0, st_>>>(changed, words_, nxt_, est_.p, P_, m_, alpha_,
+                                                  g_->out_deg.p, ctr_.p);
+      PLATO_LAUNCHED("k_hll_finish");
+    }
+    std::swap(cur_, nxt_);
+    return read_counters(n_changed, deg_changed);
+  }
+
   // One spread epoch over `dir` (rows = candidates, sources tested in `active`).
   int spread(const hll_direction& dir, const uint32_t* active, uint32_t* covered, uint32_t* next,
              unsigned long long* n, unsigned long long* deg) {
@@ -996,9 +1143,13 @@ int hyperanf_impl(plato_graph* g, const plato_hyperanf_opts* o, const plato_dual
   uint32_t* chg = h.bits(1);
   bool first = true;
   for (uint32_t it = 0; it < iterations; ++it) {
-    record_mode(st, is_push(active_edges, E, thr));
+    const bool push = is_push(active_edges, E, thr);
+    record_mode(st, push);
     unsigned long long n = 0, deg = 0;
-    PLATO_TRY(h.epoch(in_dir, first ? nullptr : act, nullptr, first ? nullptr : act, chg, &n, &deg));
+    if (push)  // the changed rows scatter (the same registers as the gather, at the cost of the actives)
+      PLATO_TRY(h.epoch_push(first ? nullptr : act, nullptr, first ? nullptr : act, chg, &n, &deg));
+    else
+      PLATO_TRY(h.epoch(in_dir, first ? nullptr : act, nullptr, first ? nullptr : act, chg, &n, &deg));
     PLATO_TRY(h.sum_estimates(&anf));
     if (anf - anfs.back() < DBL_EPSILON) break;  // hyperanf.hpp:185-187
     anfs.push_back(anf);
@@ -1090,8 +1241,11 @@ int nstep_impl(plato_graph* g, const plato_nstep_opts* o, const plato_dualmode_o
       const bool push = is_push(ae, E, thr);
       record_mode(st, push);
       const uint32_t* stale = first ? nullptr : act;
-      if (push || !prop_reversed) {
-        // forward: push from the actives, or a forward pull (same registers)
+      if (push) {
+        // the actives scatter forward (also when the phase is reversed)
+        PLATO_TRY(h.epoch_push(act, covered, stale, chg, &actives, &ae));
+      } else if (!prop_reversed) {
+        // forward pull from the actives (the registers of a pull from every in-neighbour)
         PLATO_TRY(h.epoch(fwd, act, covered, stale, chg, &actives, &ae));
       } else {
         // reversed pull: every out-neighbour (rows outside `covered` are empty)
