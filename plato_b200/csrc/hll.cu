@@ -39,6 +39,9 @@
 // rows that changed gives the same registers as merging every in-neighbour
 // whenever push and pull walk the same direction (any unchanged row was
 // merged in an earlier epoch), and it is exactly the push slot's rule.
+// Push epochs (few changed rows) scatter those rows over their out-edges
+// instead (k_hll_scatter), so their cost follows the actives' edges rather
+// than every row's sources.
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
