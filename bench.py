@@ -497,6 +497,25 @@ def suite_wpr(pb):
             "timing": "host clock around plato_weighted_pagerank (20 epochs, host output), median of 3"}
 
 
+def suite_trustrank(pb):
+    """TrustRank with seed selection by inverse PageRank (trustrank.hpp) on
+    RMAT s22 ef16 seed 4, a seeded 10% of the vertices good, 100 seeds."""
+    V, s, d = pb.rmat(22, 16, 4)
+    g = pb.Graph(V, s, d, is_directed=True)
+    good = np.random.default_rng(4).random(V) < 0.1
+    g.trustrank(good, 100, 0.85, 100, 0, 0.001)
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        _, seeds, st = g.trustrank(good, 100, 0.85, 100, 0, 0.001)
+        times.append(time.perf_counter() - t0)
+    g.close()
+    return {"workload": "trustrank_rmat_s22_ef16_seed4_good10pct", "vertices": V, "edges": int(s.size),
+            "ms_median": float(np.median(times)) * 1e3, "seeds": int(seeds.size),
+            "trust_epochs": st.iterations,
+            "timing": "host clock around plato_trustrank (selection PageRank + trust PPR, ranks to host), median of 3"}
+
+
 def suite_ppr_single(pb):
     """Single-source PPR on RMAT s24 seed 3 until L1 delta < 1e-7, both engines."""
     V, s, d = pb.rmat(24, 16, 3)
@@ -620,7 +639,8 @@ def run_suite(args):
     import torch  # noqa: F401  (CUDA context for the library)
     import plato_b200 as pb
     res = {"suite": True}
-    for name, fn in (("bfs", suite_bfs), ("cc", suite_cc), ("hll", suite_hll), ("wpr", suite_wpr),
+    for name, fn in (("bfs", suite_bfs), ("cc", suite_cc), ("trustrank", suite_trustrank), ("hll", suite_hll),
+                     ("wpr", suite_wpr),
                      ("ppr_single", suite_ppr_single),
                      ("ppr_batch", suite_batch), ("serving", suite_serving)):
         if args.only and name not in args.only.split(","):
@@ -643,7 +663,7 @@ def main():
                     help="RMAT scale (smaller values are for profiling captures only)")
     ap.add_argument("--suite", action="store_true",
                     help="also measure BFS, single PPR, batched PPR and serving (one JSON line each)")
-    ap.add_argument("--only", default="", help="with --suite: comma list of bfs,cc,hll,wpr,ppr_single,ppr_batch,serving")
+    ap.add_argument("--only", default="", help="with --suite: comma list of bfs,cc,trustrank,hll,wpr,ppr_single,ppr_batch,serving")
     ap.add_argument("--quick", action="store_true", help="with --suite: one small batch (profiling)")
     args = ap.parse_args()
     globals()["SCALE"] = args.scale

@@ -46,6 +46,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include <cstdint>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -82,6 +83,42 @@ inline void check_cuda(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Device memory of the engine (states, bitmaps, work lists, scratch) comes
+// from a stream-ordered pool on the legacy default stream, where the
+// engine's kernels run: a freed block returns to the pool without a
+// device-wide synchronisation, and the next engine, state or bitmap reuses
+// it.  The pool keeps up to kPoolKeepBytes of freed memory per device.
+constexpr uint64_t kPoolKeepBytes = 1ull << 30;
+
+inline cudaMemPool_t engine_pool() {
+  static cudaMemPool_t pools[64] = {};
+  static std::mutex mu;
+  int dev = 0;
+  check_cuda(cudaGetDevice(&dev), "engine pool: device");
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev < 0 || dev >= 64) throw std::runtime_error("engine pool: device index out of range");
+  if (!pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    check_cuda(cudaMemPoolCreate(&pools[dev], &props), "engine pool: create");
+    uint64_t keep = kPoolKeepBytes;
+    check_cuda(cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep),
+               "engine pool: release threshold");
+  }
+  return pools[dev];
+}
+
+template <typename T>
+inline void dev_alloc(T** p, size_t bytes, const char* what) {
+  check_cuda(cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes ? bytes : 1, engine_pool(), 0), what);
+}
+
+inline void dev_free(void* p) {
+  if (p) cudaFreeAsync(p, 0);
+}
+
 // Out-edge view usable inside device functors (bcsr_t::neighbours, bcsr.hpp:225-240).
 struct out_edges_view {
   const uint64_t* off;
@@ -97,7 +134,7 @@ class bitmap_t {
  public:
   bitmap_t() = default;
   explicit bitmap_t(uint32_t n) : n_(n) {
-    check_cuda(cudaMalloc(&w_, words() * sizeof(uint32_t)), "bitmap alloc");
+    dev_alloc(&w_, words() * sizeof(uint32_t), "bitmap alloc");
     clear();
   }
   bitmap_t(bitmap_t&& o) noexcept : w_(o.w_), n_(o.n_) { o.w_ = nullptr; }
@@ -109,7 +146,7 @@ class bitmap_t {
   bitmap_t(const bitmap_t&) = delete;
   bitmap_t& operator=(const bitmap_t&) = delete;
   ~bitmap_t() {
-    if (w_) cudaFree(w_);
+    dev_free(w_);
   }
   size_t words() const { return (static_cast<size_t>(n_) + 31) / 32; }
   void clear() { check_cuda(cudaMemset(w_, 0, words() * 4), "bitmap clear"); }
@@ -143,7 +180,7 @@ class dense_state_t {
  public:
   dense_state_t() = default;
   explicit dense_state_t(uint32_t n) : n_(n) {
-    check_cuda(cudaMalloc(&p_, sizeof(T) * (n ? n : 1)), "state alloc");
+    dev_alloc(&p_, sizeof(T) * (n ? n : 1), "state alloc");
   }
   dense_state_t(dense_state_t&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr; }
   dense_state_t& operator=(dense_state_t&& o) noexcept {
@@ -154,7 +191,7 @@ class dense_state_t {
   dense_state_t(const dense_state_t&) = delete;
   dense_state_t& operator=(const dense_state_t&) = delete;
   ~dense_state_t() {
-    if (p_) cudaFree(p_);
+    dev_free(p_);
   }
   T* data() const { return p_; }
   uint32_t size() const { return n_; }
@@ -311,12 +348,12 @@ void dense_state_t<T>::fill(const T& v) {
 
 inline uint64_t bitmap_t::count() const {
   unsigned long long* d = nullptr;
-  check_cuda(cudaMalloc(&d, sizeof(*d)), "count alloc");
-  cudaMemset(d, 0, sizeof(*d));
+  dev_alloc(&d, sizeof(*d), "count alloc");
+  check_cuda(cudaMemsetAsync(d, 0, sizeof(*d), 0), "count clear");
   detail::k_popc<<<296, 256>>>(w_, words(), d);
   unsigned long long h = 0;
   check_cuda(cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost), "count read");
-  cudaFree(d);
+  dev_free(d);
   return h;
 }
 
@@ -330,10 +367,10 @@ class dualmode_engine_t {
   dualmode_engine_t(const dualmode_engine_t&) = delete;
   dualmode_engine_t& operator=(const dualmode_engine_t&) = delete;
   ~dualmode_engine_t() {
-    if (chunks_) cudaFree(chunks_);
-    if (queue_) cudaFree(queue_);
-    if (counters_) cudaFree(counters_);
-    if (result_) cudaFree(result_);
+    dev_free(chunks_);
+    dev_free(queue_);
+    dev_free(counters_);
+    dev_free(result_);
   }
 
   const plato_graph_info& graph_info() const { return info_; }
@@ -419,38 +456,38 @@ class dualmode_engine_t {
   // scan for the start of each column's chunks, then the fill).
   void ensure_chunks() {
     if (chunks_ && chunks_reversed_ == reversed_) return;
-    if (chunks_) cudaFree(chunks_);
+    dev_free(chunks_);
     chunks_ = nullptr;
     const uint32_t V = view_.vertices;
     uint64_t* cnt = nullptr;
     uint64_t* start = nullptr;
     void* tmp = nullptr;
     size_t tmp_bytes = 0;
-    check_cuda(cudaMalloc(&cnt, 8ull * (V ? V : 1)), "chunks");
-    check_cuda(cudaMalloc(&start, 8ull * (V + 1)), "chunks");
+    dev_alloc(&cnt, 8ull * (V ? V : 1), "chunks");
+    dev_alloc(&start, 8ull * (V + 1), "chunks");
     detail::k_count_chunks<<<grid(V), 256>>>(in_off(), V, cnt);
     check_cuda(cudaMemset(start, 0, sizeof(uint64_t)), "chunks");
     check_cuda(cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, cnt, start + 1, static_cast<int64_t>(V)),
                "chunks");
-    check_cuda(cudaMalloc(&tmp, tmp_bytes ? tmp_bytes : 1), "chunks");
+    dev_alloc(&tmp, tmp_bytes, "chunks");
     check_cuda(cub::DeviceScan::InclusiveSum(tmp, tmp_bytes, cnt, start + 1, static_cast<int64_t>(V)),
                "chunks");
     uint64_t total = 0;
     check_cuda(cudaMemcpy(&total, start + V, sizeof(total), cudaMemcpyDeviceToHost), "chunks");
     nchunks_ = total;
-    check_cuda(cudaMalloc(&chunks_, sizeof(uint2) * (nchunks_ ? nchunks_ : 1)), "chunks");
+    dev_alloc(&chunks_, sizeof(uint2) * (nchunks_ ? nchunks_ : 1), "chunks");
     detail::k_fill_chunks<<<grid(V), 256>>>(in_off(), V, start, chunks_);
-    check_cuda(cudaDeviceSynchronize(), "chunks");
-    cudaFree(tmp);
-    cudaFree(cnt);
-    cudaFree(start);
+    check_cuda(cudaGetLastError(), "chunks");
+    dev_free(tmp);
+    dev_free(cnt);
+    dev_free(start);
     chunks_reversed_ = reversed_;
   }
 
   void compact(bitmap_t& actives, uint64_t* n, uint64_t* active_edges) {
     const uint32_t V = view_.vertices;
-    if (!queue_) check_cuda(cudaMalloc(&queue_, 4ull * (V ? V : 1)), "queue");
-    if (!counters_) check_cuda(cudaMalloc(&counters_, 16), "counters");
+    if (!queue_) dev_alloc(&queue_, 4ull * (V ? V : 1), "queue");
+    if (!counters_) dev_alloc(&counters_, 16, "counters");
     check_cuda(cudaMemset(counters_, 0, 16), "counters");
     const uint32_t* deg = reversed_ ? view_.in_degree : view_.out_degree;
     detail::k_compact<<<grid(V), 256>>>(actives.data(), V, deg, queue_, counters_);
@@ -472,7 +509,7 @@ class dualmode_engine_t {
 
   template <typename R>
   R* result_buf() {
-    if (!result_) check_cuda(cudaMalloc(&result_, 16), "result");
+    if (!result_) dev_alloc(&result_, 16, "result");
     check_cuda(cudaMemset(result_, 0, 16), "result");
     return reinterpret_cast<R*>(result_);
   }

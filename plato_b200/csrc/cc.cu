@@ -41,18 +41,26 @@ __global__ void k_cc_init(vid_t* labels, const vid_t* __restrict__ to_ext, uint3
 }
 
 // cnt[label] = vertices carrying it; roots (label == own caller id) count
-// the components; best = max over labels of (count << 32 | ~label).
+// the components; best = max over labels of (count << 32 | ~label).  Lanes
+// of a warp holding the same label add once for all of them (a large
+// component's label would otherwise take one atomic per vertex on a single
+// counter).
 __global__ void k_cc_count(const vid_t* __restrict__ labels, const vid_t* __restrict__ to_ext,
                            uint32_t V, uint32_t* cnt, unsigned long long* roots) {
+  const unsigned lane = threadIdx.x & 31;
   unsigned long long r = 0;
-  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
-       v += (uint64_t)gridDim.x * blockDim.x) {
-    const vid_t l = labels[v];
-    atomicAdd(&cnt[l], 1u);
-    r += (l == (to_ext ? to_ext[v] : static_cast<vid_t>(v)));
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;  // a multiple of 32
+  // the warp stays together: the trip count follows its first lane
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v - lane < V; v += stride) {
+    const bool valid = v < V;
+    const vid_t l = valid ? labels[v] : 0xFFFFFFFFu;
+    const unsigned same = __match_any_sync(0xFFFFFFFFu, l);
+    if (valid && lane == static_cast<unsigned>(__ffs(same) - 1))
+      atomicAdd(&cnt[l], static_cast<uint32_t>(__popc(same)));
+    r += (valid && l == (to_ext ? to_ext[v] : static_cast<vid_t>(v))) ? 1ull : 0ull;
   }
   r = warp_sum(r);
-  if ((threadIdx.x & 31) == 0 && r) atomicAdd(roots, r);
+  if (lane == 0 && r) atomicAdd(roots, r);
 }
 
 __global__ void k_cc_major(const uint32_t* __restrict__ cnt, uint32_t V, unsigned long long* best) {
@@ -152,8 +160,8 @@ int cc_impl(plato_graph* g, const plato_dualmode_opts* eo, plato_vid_t* labels_o
   if (summary) {
     uint32_t* cnt = nullptr;
     unsigned long long* acc = nullptr;  // [0] roots, [1] best, [2] major edges
-    check_cuda(cudaMalloc(&cnt, 4ull * (V ? V : 1)), "cc counts");
-    check_cuda(cudaMalloc(&acc, 3 * sizeof(unsigned long long)), "cc summary");
+    dev_alloc(&cnt, 4ull * (V ? V : 1), "cc counts");
+    dev_alloc(&acc, 3 * sizeof(unsigned long long), "cc summary");
     int rc = PLATO_OK;
     try {
       check_cuda(cudaMemset(cnt, 0, 4ull * V), "cc counts");
@@ -179,8 +187,8 @@ int cc_impl(plato_graph* g, const plato_dualmode_opts* eo, plato_vid_t* labels_o
     } catch (const std::exception& e) {
       rc = set_error(PLATO_ECUDA, e.what());
     }
-    cudaFree(cnt);
-    cudaFree(acc);
+    dev_free(cnt);
+    dev_free(acc);
     if (rc != PLATO_OK) return rc;
   }
   if (labels_out) {

@@ -76,7 +76,7 @@ std::vector<double> selection_pagerank(plato_graph* g, bool inverse) {
   auto curt = engine.alloc_v_state<double>();
   auto next = engine.alloc_v_state<double>();
   double* delta = nullptr;
-  check_cuda(cudaMalloc(&delta, sizeof(double)), "trustrank delta");
+  dev_alloc(&delta, sizeof(double), "trustrank delta");
   try {
     k_tr_init<<<grid_for(V, 256), 256>>>(curt.data(), deg, V);
     check_cuda(cudaGetLastError(), "k_tr_init");
@@ -106,10 +106,10 @@ std::vector<double> selection_pagerank(plato_graph* g, bool inverse) {
       std::swap(curt, next);
     }
   } catch (...) {
-    cudaFree(delta);
+    dev_free(delta);
     throw;
   }
-  cudaFree(delta);
+  dev_free(delta);
   return engine.to_host(curt);
 }
 
