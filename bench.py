@@ -384,7 +384,24 @@ def suite_bfs(pb, roots_n=64):
     return {"workload": "bfs_rmat_s22_ef16_seed2_sym", "vertices": V, "undirected_edges": int(s.size),
             "roots": roots_n, "gteps_harmonic_mean": hm / 1e9,
             "ms_median": float(np.median(times)) * 1e3, "mode_trace_example": modes[0],
-            "timing": "host clock around plato_bfs (levels not copied back)"}
+            "timing": "host clock around plato_bfs (levels not copied back)",
+            "cpu_baseline": cpu_bfs_sample(V, s, d, roots[:4], deg)}
+
+
+def cpu_bfs_sample(V, s, d, roots, deg):
+    """The oracle's C/OpenMP BFS (the reference's dual-mode rules) on the host
+    cores, for a few of the same roots: harmonic-mean GTEPS."""
+    import oracle
+    ref = oracle.RefGraph(V, s, d, False)
+    teps = []
+    for r in roots:
+        t0 = time.perf_counter()
+        lev, _, _, _, _ = ref.bfs(int(r), 0.05)
+        dt = time.perf_counter() - t0
+        teps.append(int(deg[lev != 0xFFFFFFFF].sum()) // 2 / dt)
+    ref.close()
+    return {"gteps_harmonic_mean": len(teps) / sum(1.0 / t for t in teps) / 1e9, "cores": oracle.max_threads(),
+            "kind": "port", "sample": f"{len(roots)} of the same roots, oracle ref_cpu.c"}
 
 
 def suite_cc(pb):
@@ -530,6 +547,16 @@ def suite_ppr_single(pb):
         dt = time.perf_counter() - t0
         out[name] = {"ms": dt * 1e3, "iterations": st.iterations, "push_iterations": st.push_iterations}
     g.close()
+    import oracle  # CPU baseline: a bounded sample of the same query's pull epochs
+    ref = oracle.RefGraph(V, s, d, True)
+    t0 = time.perf_counter()
+    ref.ppr(src, 3, 0.85, 0.0)
+    per_epoch = (time.perf_counter() - t0) / 3
+    ref.close()
+    out["cpu_baseline"] = {"ms_per_epoch": per_epoch * 1e3,
+                           "query_ms_at_gpu_epochs": per_epoch * 1e3 * out["pull"]["iterations"],
+                           "cores": oracle.max_threads(), "kind": "port",
+                           "sample": "3 pull epochs of the same query, oracle ref_cpu.c (FP64)"}
     return out
 
 
@@ -581,6 +608,14 @@ def suite_batch(pb, plain_n=16, quick=False):
           for q in range(plain_n)]
     res["l1_batch_vs_plain_max"] = max(l1)
     g.close()
+    import oracle  # CPU baseline: the first query, whole, on the host cores
+    ref = oracle.RefGraph(V, s, d, True)
+    t0 = time.perf_counter()
+    _, ep, _ = ref.seedset_ppr(sets[0], 300, 0.85, 1e-6)
+    dt = time.perf_counter() - t0
+    ref.close()
+    res["cpu_baseline"] = {"qps": 1.0 / dt, "epochs": ep, "cores": oracle.max_threads(), "kind": "port",
+                           "sample": "query 0 of the same seed sets, oracle ref_cpu.c (FP64)"}
     return res
 
 
