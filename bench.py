@@ -146,20 +146,23 @@ def pull_bins(V: int, dst) -> dict:
 
 def cpu_pagerank_sample(V, src, dst, target_s=15.0):
     """Oracle (reference restatement) PageRank epochs on all host threads,
-    sized to ~target_s seconds; returns (GTEPS, epochs, seconds, threads, E)."""
+    sized to ~target_s seconds; returns (GTEPS, epochs, seconds, threads, E,
+    FP64 ranks after ITERATIONS epochs in reference units)."""
     import oracle
     g = oracle.RefGraph(V, src, dst, True)
     E = g.stored_edges
     t0 = time.perf_counter()
     g.pagerank(1, DAMPING, 0.0)
     t1 = time.perf_counter() - t0
-    n = int(max(1, min(20, target_s / max(t1, 1e-3))))
+    n = int(max(1, min(ITERATIONS, target_s / max(t1, 1e-3))))
     t0 = time.perf_counter()
-    g.pagerank(n, DAMPING, 0.0)
+    ranks, _, _ = g.pagerank(n, DAMPING, 0.0)
     dt = time.perf_counter() - t0
+    if n != ITERATIONS:
+        ranks, _, _ = g.pagerank(ITERATIONS, DAMPING, 0.0)
     thr = oracle.max_threads()
     g.close()
-    return E * n / dt / 1e9, n, dt, thr, E
+    return E * n / dt / 1e9, n, dt, thr, E, ranks
 
 
 def run_reference(args):
@@ -339,10 +342,14 @@ def run_plato(args):
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        gteps, n, dt, thr, _ = cpu_pagerank_sample(V, src, dst)
+        gteps, n, dt, thr, _, want = cpu_pagerank_sample(V, src, dst)
         line["cpu_baseline"] = {"value": gteps, "unit": "GTEPS", "cores": thr, "kind": "port",
                                 "sample": f"{n} PageRank epochs on the same s{SCALE} graph "
                                           f"({dt:.1f} s, oracle ref_cpu.c, FP64, OpenMP)"}
+        err = np.abs(host_out.numpy().astype(np.float64) - want / V)
+        line["parity"] = {"vs": f"oracle ref_cpu.c FP64, {ITERATIONS} epochs, reference ranks / V",
+                          "l1": float(err.sum()), "max_abs": float(err.max()), "tolerance_l1": 1e-6,
+                          "ok": bool(err.sum() <= 1e-6)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     g.close()
@@ -369,9 +376,11 @@ def suite_bfs(pb, roots_n=64):
     rng = np.random.default_rng(2)
     roots = rng.choice(np.flatnonzero(deg > 0), roots_n, replace=False)
     g.bfs(int(roots[0]), parents=False, levels=False)
-    teps, times, modes = [], [], []
+    teps, times, modes, kept = [], [], [], []
     for r in roots:
         lev, _, st = g.bfs(int(r), parents=False)
+        if len(kept) < 4:
+            kept.append(lev)
         m = int(deg[lev != pb.PLATO_LEVEL_UNREACHED].sum()) // 2
         t0 = time.perf_counter()
         _, _, st = g.bfs(int(r), parents=False, levels=False)
@@ -385,23 +394,26 @@ def suite_bfs(pb, roots_n=64):
             "roots": roots_n, "gteps_harmonic_mean": hm / 1e9,
             "ms_median": float(np.median(times)) * 1e3, "mode_trace_example": modes[0],
             "timing": "host clock around plato_bfs (levels not copied back)",
-            "cpu_baseline": cpu_bfs_sample(V, s, d, roots[:4], deg)}
+            "cpu_baseline": cpu_bfs_sample(V, s, d, roots[:len(kept)], deg, kept)}
 
 
-def cpu_bfs_sample(V, s, d, roots, deg):
+def cpu_bfs_sample(V, s, d, roots, deg, gpu_levels):
     """The oracle's C/OpenMP BFS (the reference's dual-mode rules) on the host
-    cores, for a few of the same roots: harmonic-mean GTEPS."""
+    cores, for a few of the same roots: harmonic-mean GTEPS, and whether the
+    GPU's levels for those roots equal the oracle's bit for bit."""
     import oracle
     ref = oracle.RefGraph(V, s, d, False)
-    teps = []
-    for r in roots:
+    teps, same = [], []
+    for r, mine in zip(roots, gpu_levels):
         t0 = time.perf_counter()
         lev, _, _, _, _ = ref.bfs(int(r), 0.05)
         dt = time.perf_counter() - t0
         teps.append(int(deg[lev != 0xFFFFFFFF].sum()) // 2 / dt)
+        same.append(bool(np.array_equal(lev, mine)))
     ref.close()
     return {"gteps_harmonic_mean": len(teps) / sum(1.0 / t for t in teps) / 1e9, "cores": oracle.max_threads(),
-            "kind": "port", "sample": f"{len(roots)} of the same roots, oracle ref_cpu.c"}
+            "kind": "port", "sample": f"{len(roots)} of the same roots, oracle ref_cpu.c",
+            "levels_bit_exact": all(same)}
 
 
 def suite_cc(pb):
@@ -540,23 +552,27 @@ def suite_ppr_single(pb):
     deg = np.bincount(s, minlength=V)
     src = int(np.random.default_rng(3).choice(np.flatnonzero(deg > 0)))
     out = {"workload": "ppr_rmat_s24_ef16_seed3", "src": src}
+    got = {}
     for mode, name in ((pb.PLATO_PPR_PULL, "pull"), (pb.PLATO_PPR_PUSHPULL, "pushpull")):
         g.personalized_pagerank(src, 500, 0.85, 1e-7, mode)
         t0 = time.perf_counter()
-        _, st = g.personalized_pagerank(src, 500, 0.85, 1e-7, mode)
+        got[name], st = g.personalized_pagerank(src, 500, 0.85, 1e-7, mode)
         dt = time.perf_counter() - t0
         out[name] = {"ms": dt * 1e3, "iterations": st.iterations, "push_iterations": st.push_iterations}
     g.close()
-    import oracle  # CPU baseline: a bounded sample of the same query's pull epochs
+    import oracle  # CPU baseline: the same query, whole, pull-only and push-pull
     ref = oracle.RefGraph(V, s, d, True)
-    t0 = time.perf_counter()
-    ref.ppr(src, 3, 0.85, 0.0)
-    per_epoch = (time.perf_counter() - t0) / 3
+    for pushpull, name in ((False, "pull"), (True, "pushpull")):
+        t0 = time.perf_counter()
+        want, ep, pe, _, _ = ref.ppr(src, 500, 0.85, 1e-7, pushpull)
+        dt = time.perf_counter() - t0
+        err = np.abs(got[name].astype(np.float64) - want)
+        out[name]["parity"] = {"vs": "oracle ref_cpu.c FP64", "l1": float(err.sum()),
+                               "max_abs": float(err.max()), "oracle_epochs": ep, "tolerance_l1": 1e-6}
+        out[name]["cpu_baseline"] = {"ms": dt * 1e3, "epochs": ep, "push_epochs": pe,
+                                     "cores": oracle.max_threads(), "kind": "port",
+                                     "sample": "the same query, whole, oracle ref_cpu.c (FP64)"}
     ref.close()
-    out["cpu_baseline"] = {"ms_per_epoch": per_epoch * 1e3,
-                           "query_ms_at_gpu_epochs": per_epoch * 1e3 * out["pull"]["iterations"],
-                           "cores": oracle.max_threads(), "kind": "port",
-                           "sample": "3 pull epochs of the same query, oracle ref_cpu.c (FP64)"}
     return out
 
 
@@ -611,11 +627,14 @@ def suite_batch(pb, plain_n=16, quick=False):
     import oracle  # CPU baseline: the first query, whole, on the host cores
     ref = oracle.RefGraph(V, s, d, True)
     t0 = time.perf_counter()
-    _, ep, _ = ref.seedset_ppr(sets[0], 300, 0.85, 1e-6)
+    want, ep, _ = ref.seedset_ppr(sets[0], 300, 0.85, 1e-6)
     dt = time.perf_counter() - t0
     ref.close()
     res["cpu_baseline"] = {"qps": 1.0 / dt, "epochs": ep, "cores": oracle.max_threads(), "kind": "port",
                            "sample": "query 0 of the same seed sets, oracle ref_cpu.c (FP64)"}
+    err = np.abs(chk["ranks"][0].astype(np.float64) - want)
+    res["parity_query0"] = {"vs": "oracle ref_cpu.c FP64", "l1": float(err.sum()), "max_abs": float(err.max()),
+                            "epochs": int(chk["iterations"][0]), "oracle_epochs": ep, "tolerance_l1": 1e-6}
     return res
 
 

@@ -260,7 +260,8 @@ static int rank_loop(const ref_graph* g, int tele_kind, uint32_t src, const uint
   double* curt = (double*)malloc((size_t)V * 8);
   double* next = (double*)malloc((size_t)V * 8);
   uint64_t* actives = (uint64_t*)calloc(bm_words(V), 8);
-  if (!curt || !next || !actives) return 2;
+  uint64_t* walk = (uint64_t*)malloc(bm_words(V) * 8);
+  if (!curt || !next || !actives || !walk) return 2;
   const uint32_t* odeg = g->out_degree;
   /* init */
 #pragma omp parallel for schedule(static)
@@ -293,11 +294,20 @@ static int rank_loop(const ref_graph* g, int tele_kind, uint32_t src, const uint
     if (do_pull) {
       pull_sum(g, curt, next);
     } else {
-      /* broadcast over active vertices; slot scatters to out-neighbours */
+      /* broadcast over active vertices; slot scatters to out-neighbours and
+       * marks them active (personalized_pagerank.hpp:225-239).  The slot sets
+       * bits in the bitmap the broadcast is scanning, from other threads, so
+       * in the reference a vertex reached in this epoch may or may not be
+       * broadcast in this epoch too, by thread timing.  Its rank is still 0,
+       * so the ranks are the same either way; only the active-edge count of
+       * the next switch test can differ.  This restatement takes the one
+       * order that does not depend on timing: the epoch broadcasts the
+       * actives it started with. */
       const uint64_t words = bm_words(V);
+      memcpy(walk, actives, words * 8);
 #pragma omp parallel for schedule(dynamic, 64)
       for (int64_t w = 0; w < (int64_t)words; ++w) {
-        uint64_t bits = actives[w];
+        uint64_t bits = walk[w];
         while (bits) {
           const int b = __builtin_ctzll(bits);
           bits &= bits - 1;
@@ -341,6 +351,7 @@ static int rank_loop(const ref_graph* g, int tele_kind, uint32_t src, const uint
   free(curt);
   free(next);
   free(actives);
+  free(walk);
   return 0;
 }
 

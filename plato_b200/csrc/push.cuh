@@ -174,8 +174,13 @@ inline int frontier_active_edges(push_frontier& f, cudaStream_t st, uint64_t* ac
 }
 
 // PPR push epoch (personalized_pagerank.hpp:225-239): every member u adds
-// x[u] to y[dst] for its out-edges and marks dst active (same frontier; a
-// vertex reached this epoch holds x == 0, so walking it now or later is the same).
+// x[u] to y[dst] for its out-edges and marks dst active in the same frontier.
+// The epoch walks the members it started with (the chunk count read before
+// the launch).  In the reference the slot sets bits in the bitmap the
+// broadcast is still scanning, so a vertex reached this epoch may be walked
+// in it or not by thread timing; it holds x == 0, so the ranks are the same,
+// and the order taken here is the one that leaves the active-edge count, and
+// so the push/pull switch epoch, independent of timing.
 static __global__ void __launch_bounds__(256) k_ppr_push(frontier_view f, unsigned long long nchunks,
                                                   const uint64_t* __restrict__ out_off,
                                                   const uint32_t* __restrict__ out_adj,
