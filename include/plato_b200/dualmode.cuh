@@ -58,7 +58,7 @@ namespace plato_b200 {
 using vid_t = uint32_t;
 using eid_t = uint64_t;
 
-constexpr uint32_t kPullChunk = 256;
+constexpr uint32_t kPullChunk = 64;
 
 struct adj_unit_t {  // adj_unit_t<empty_t> (plato/graph/base.hpp)
   vid_t neighbour_;
@@ -416,6 +416,18 @@ class dualmode_engine_t {
                                                      slot, res);
     check_cuda(cudaGetLastError(), "pull launch");
     return read_result<R>(res);
+  }
+
+  // pull only, the sum of the slot returns added into *d_result (device
+  // memory, not cleared here) instead of read back: the call does not
+  // synchronise, so a loop whose epochs are decided on the device can be
+  // enqueued back to back.
+  template <typename MSG, typename R, typename PULL_SIGNAL, typename PULL_SLOT>
+  void foreach_edges_device(PULL_SIGNAL signal, PULL_SLOT slot, R* d_result) {
+    ensure_chunks();
+    detail::k_pull<MSG, R><<<grid(nchunks_), 256>>>(chunks_, nchunks_, in_off(), in_adj(), signal,
+                                                     slot, d_result);
+    check_cuda(cudaGetLastError(), "pull launch");
   }
 
   // push only (dualmode.hpp:311-322)

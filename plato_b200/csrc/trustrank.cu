@@ -40,9 +40,12 @@ __global__ void k_tr_init(double* x, const uint32_t* __restrict__ deg, uint32_t 
 }
 
 // pagerank.hpp:118-135: r = (1-d) + d*y; non-final epochs divide by the degree
-// and sum |x' - x| * deg into *delta.
+// and sum |x' - x| * deg into *delta.  The epoch is final when it is the last
+// one or when ctrl[1] says so; nothing runs once ctrl[0] is set.
 __global__ void k_tr_update(double* n, const double* __restrict__ c, const uint32_t* __restrict__ deg,
-                            uint32_t V, double d, int last, double* delta) {
+                            uint32_t V, double d, int last_epoch, double* delta, const uint32_t* ctrl) {
+  if (ctrl[0]) return;
+  const bool last = last_epoch || ctrl[1];
   double dl = 0.0;
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
        v += (uint64_t)gridDim.x * blockDim.x) {
@@ -61,6 +64,30 @@ __global__ void k_tr_update(double* n, const double* __restrict__ c, const uint3
   if ((threadIdx.x & 31) == 0 && dl != 0.0) atomicAdd(delta, dl);
 }
 
+// next.fill(0) of the epoch, skipped like the rest once the final epoch has
+// run (the buffer it would clear may hold the result).
+__global__ void k_tr_zero(double* n, uint32_t V, const uint32_t* ctrl) {
+  if (ctrl[0]) return;
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+       v += (uint64_t)gridDim.x * blockDim.x)
+    n[v] = 0.0;
+}
+
+// The eps early exit of pagerank.hpp:137-139 decided on the device, so the
+// host enqueues every epoch without waiting: after a non-final epoch with
+// delta < eps the next epoch is the final one (ctrl[1]); after the final
+// epoch ctrl[0] stops the rest and ctrl[2] records which epoch it was.
+__global__ void k_tr_control(double* delta, double eps, uint32_t epoch, int last_epoch, uint32_t* ctrl) {
+  if (ctrl[0]) return;
+  if (last_epoch || ctrl[1]) {
+    ctrl[0] = 1;
+    ctrl[2] = epoch;
+  } else if (*delta < eps) {
+    ctrl[1] = 1;
+  }
+  *delta = 0.0;
+}
+
 // Ranks (caller-id order) of the reference's default PageRank on the graph
 // (transposed when `inverse`).
 std::vector<double> selection_pagerank(plato_graph* g, bool inverse) {
@@ -73,20 +100,29 @@ std::vector<double> selection_pagerank(plato_graph* g, bool inverse) {
   // out-degrees of the structure the pull walks: in-degrees when transposed
   const uint32_t* deg = inverse ? view.in_degree : view.out_degree;
   const uint32_t V = engine.vertices();
-  auto curt = engine.alloc_v_state<double>();
-  auto next = engine.alloc_v_state<double>();
+  dense_state_t<double> x[2] = {engine.alloc_v_state<double>(), engine.alloc_v_state<double>()};
   double* delta = nullptr;
+  uint32_t* ctrl = nullptr;
+  int* unused = nullptr;
   dev_alloc(&delta, sizeof(double), "trustrank delta");
+  uint32_t final_epoch = 0;
   try {
-    k_tr_init<<<grid_for(V, 256), 256>>>(curt.data(), deg, V);
+    dev_alloc(&ctrl, 3 * sizeof(uint32_t), "trustrank control");
+    dev_alloc(&unused, sizeof(int), "trustrank slot sum");
+    check_cuda(cudaMemset(delta, 0, sizeof(double)), "trustrank delta");
+    check_cuda(cudaMemset(ctrl, 0, 3 * sizeof(uint32_t)), "trustrank control");
+    k_tr_init<<<grid_for(V, 256), 256>>>(x[0].data(), deg, V);
     check_cuda(cudaGetLastError(), "k_tr_init");
     count_launch();
     for (uint32_t epoch = 0; epoch < kIterations; ++epoch) {
-      next.fill(0.0);
-      const double* c = curt.data();
-      double* n = next.data();
-      engine.foreach_edges<double, int>(
-          [c] __device__(const auto& context, vid_t v_i, const adj_unit_list_t& adjs) {
+      const double* c = x[epoch & 1].data();
+      double* n = x[(epoch & 1) ^ 1].data();
+      k_tr_zero<<<grid_for(V, 256), 256>>>(n, V, ctrl);
+      check_cuda(cudaGetLastError(), "k_tr_zero");
+      const uint32_t* done = ctrl;
+      engine.foreach_edges_device<double, int>(
+          [c, done] __device__(const auto& context, vid_t v_i, const adj_unit_list_t& adjs) {
+            if (*done) return;
             double rank_sum = 0.0;
             for (auto it = adjs.begin_; adjs.end_ != it; ++it) rank_sum += c[it->neighbour_];
             context.send(mepa_ag_message_t<double>{v_i, rank_sum});
@@ -94,23 +130,26 @@ std::vector<double> selection_pagerank(plato_graph* g, bool inverse) {
           [n] __device__(int, mepa_ag_message_t<double>& msg) -> int {
             atomicAdd(n + msg.v_i_, msg.message_);  // write_add (atomic.hpp:97-104)
             return 0;
-          });
-      const bool last = epoch + 1 == kIterations;
-      check_cuda(cudaMemset(delta, 0, sizeof(double)), "trustrank delta");
-      k_tr_update<<<grid_for(V, 256), 256>>>(n, c, deg, V, kDamping, last ? 1 : 0, delta);
+          },
+          unused);
+      const int last = epoch + 1 == kIterations ? 1 : 0;
+      k_tr_update<<<grid_for(V, 256), 256>>>(n, c, deg, V, kDamping, last, delta, ctrl);
       check_cuda(cudaGetLastError(), "k_tr_update");
-      count_launch(3);
-      double h = 0.0;
-      check_cuda(cudaMemcpy(&h, delta, sizeof(double), cudaMemcpyDeviceToHost), "trustrank delta");
-      if (!last && h < kEps) epoch = kIterations - 2;  // pagerank.hpp:137-139
-      std::swap(curt, next);
+      k_tr_control<<<1, 1>>>(delta, kEps, epoch, last, ctrl);
+      check_cuda(cudaGetLastError(), "k_tr_control");
+      count_launch(5);
     }
+    check_cuda(cudaMemcpy(&final_epoch, ctrl + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost), "trustrank control");
   } catch (...) {
     dev_free(delta);
+    dev_free(ctrl);
+    dev_free(unused);
     throw;
   }
   dev_free(delta);
-  return engine.to_host(curt);
+  dev_free(ctrl);
+  dev_free(unused);
+  return engine.to_host(x[(final_epoch & 1) ^ 1]);
 }
 
 int select_seeds(plato_graph* g, const plato_trustrank_opts* o, const uint8_t* good,
