@@ -136,3 +136,38 @@ def test_cc_oracle_matches_reference_test_labelling(golden):
     lab = fp64.cc_labels(V, s, d, False)
     assert (lab == fp64.cc_components_bfs(V, s, d)).all()
     assert (lab <= np.arange(V)).all()
+
+
+def _switch_epoch(V, s, d, src):
+    """Push epochs of dual-mode PPR from `src` when every push epoch walks the
+    actives it started with: the actives after k push epochs are the vertices
+    within k hops, and the switch comes at the first k whose out-degree sum
+    exceeds edges / 20 (personalized_pagerank.hpp:184-205)."""
+    deg = np.bincount(s, minlength=V).astype(np.int64)
+    order = np.argsort(s, kind="stable")
+    off = np.zeros(V + 1, np.int64)
+    off[1:] = np.cumsum(deg)
+    nbr = d[order]
+    act = np.zeros(V, bool)
+    act[src] = True
+    k = 0
+    while int(deg[act].sum()) <= s.size // 20:
+        members = np.flatnonzero(act)
+        reach = np.concatenate([nbr[off[u]:off[u + 1]] for u in members]) if members.size else []
+        act[reach] = True
+        k += 1
+    return k
+
+
+def test_oracle_push_epochs_follow_the_epoch_start_actives():
+    """A vertex reached in a push epoch is walked from the next epoch on, so
+    the switch epoch is a function of the graph alone (the same on every run
+    and thread count) and equals the hop-ball recount above."""
+    import plato_b200 as pb
+    V, s, d = pb.rmat(16, 16, 3)
+    g = RefGraph(V, s, d, True)
+    deg = g.out_degrees()
+    for src in np.flatnonzero(deg > 0)[[3, 100, 2000]]:
+        want = _switch_epoch(V, s, d, int(src))
+        runs = {g.ppr(int(src), 10, 0.85, 0.0, True)[2] for _ in range(3)}
+        assert runs == {min(want, 10)}, (src, runs, want)
