@@ -27,6 +27,8 @@
 #include <unordered_set>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "graph.cuh"
 #include "plato_b200/dualmode.cuh"
 
@@ -88,9 +90,61 @@ __global__ void k_tr_control(double* delta, double eps, uint32_t epoch, int last
   *delta = 0.0;
 }
 
-// Ranks (caller-id order) of the reference's default PageRank on the graph
-// (transposed when `inverse`).
-std::vector<double> selection_pagerank(plato_graph* g, bool inverse) {
+// Selection ranks laid out by caller id, with the caller ids beside them.
+__global__ void k_tr_keys(const double* __restrict__ r, const uint32_t* __restrict__ to_ext, uint32_t V,
+                          double* keys, uint32_t* ids) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t e = to_ext ? to_ext[v] : static_cast<uint32_t>(v);
+    keys[e] = r[v];
+    ids[e] = e;
+  }
+}
+
+// The k caller ids of highest rank, ties by smaller id (trustrank.hpp:108-112),
+// chosen on the device: a stable descending radix sort of (rank, id) pairs
+// laid out by ascending id keeps equal ranks in id order.  Ranks are
+// positive and finite, where the radix order of doubles is their numeric
+// order.
+std::vector<uint32_t> top_ids(const double* r, const uint32_t* to_ext, uint32_t V, uint32_t k) {
+  double *ka = nullptr, *kb = nullptr;
+  uint32_t *ia = nullptr, *ib = nullptr;
+  void* tmp = nullptr;
+  size_t bytes = 0;
+  std::vector<uint32_t> out(k);
+  check_cuda(cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, ka, kb, ia, ib, static_cast<int64_t>(V)),
+             "top ids");
+  try {
+    dev_alloc(&ka, 8ull * V, "top ids");
+    dev_alloc(&kb, 8ull * V, "top ids");
+    dev_alloc(&ia, 4ull * V, "top ids");
+    dev_alloc(&ib, 4ull * V, "top ids");
+    dev_alloc(&tmp, bytes, "top ids");
+    k_tr_keys<<<grid_for(V, 256), 256>>>(r, to_ext, V, ka, ia);
+    check_cuda(cudaGetLastError(), "k_tr_keys");
+    count_launch();
+    check_cuda(cub::DeviceRadixSort::SortPairsDescending(tmp, bytes, ka, kb, ia, ib, static_cast<int64_t>(V)),
+               "top ids");
+    if (k) check_cuda(cudaMemcpy(out.data(), ib, 4ull * k, cudaMemcpyDeviceToHost), "top ids");
+  } catch (...) {
+    dev_free(ka);
+    dev_free(kb);
+    dev_free(ia);
+    dev_free(ib);
+    dev_free(tmp);
+    throw;
+  }
+  dev_free(ka);
+  dev_free(kb);
+  dev_free(ia);
+  dev_free(ib);
+  dev_free(tmp);
+  return out;
+}
+
+// The k caller ids of highest rank under the reference's default PageRank on
+// the graph (transposed when `inverse`).
+std::vector<uint32_t> selection_top(plato_graph* g, bool inverse, uint32_t k) {
   constexpr uint32_t kIterations = 100;
   constexpr double kDamping = 0.85, kEps = 0.001;
   dualmode_engine_t engine(g);
@@ -149,7 +203,7 @@ std::vector<double> selection_pagerank(plato_graph* g, bool inverse) {
   dev_free(delta);
   dev_free(ctrl);
   dev_free(unused);
-  return engine.to_host(x[(final_epoch & 1) ^ 1]);
+  return top_ids(x[(final_epoch & 1) ^ 1].data(), view.to_external, V, k);
 }
 
 int select_seeds(plato_graph* g, const plato_trustrank_opts* o, const uint8_t* good,
@@ -173,13 +227,8 @@ int select_seeds(plato_graph* g, const plato_trustrank_opts* o, const uint8_t* g
     std::sort(seeds->begin(), seeds->end());
     return PLATO_OK;
   }
-  const std::vector<double> rank = selection_pagerank(g, o->select_method == 0);
-  std::vector<uint32_t> order(V);
-  for (uint32_t v = 0; v < V; ++v) order[v] = v;
   const uint32_t k = std::min<uint32_t>(o->seed_num, V);
-  std::partial_sort(order.begin(), order.begin() + k, order.end(), [&](uint32_t a, uint32_t b) {
-    return rank[a] > rank[b] || (rank[a] == rank[b] && a < b);  // trustrank.hpp:108-112
-  });
+  const std::vector<uint32_t> order = selection_top(g, o->select_method == 0, k);
   for (uint32_t i = 0; i < k; ++i)
     if (is_good(order[i])) seeds->push_back(order[i]);
   std::sort(seeds->begin(), seeds->end());
