@@ -1,5 +1,6 @@
 #!/usr/bin/env python
-"""Benchmark: PageRank GTEPS on RMAT scale 24 (one B200 per process).
+"""Benchmark: PageRank GTEPS on RMAT scale 24, plus batched-PPR and serving
+queries/s (one B200 per process).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl plato|reference]
 
@@ -10,14 +11,19 @@ accumulation.  The graph (CSC+CSR, ~2.2 GB) is resident in HBM and larger
 than L2, so no L2 flush is needed between steps.
 
 Metric: GTEPS = stored edges x iterations / step time.  `value` times the
-device-output entry point (plato_pagerank_device) with the graph resident;
-`e2e` times the host-buffer C-ABI call plato_pagerank (ranks copied back to
-pinned host memory every step).  Multi-GPU runs are independent replicas
-(weak scaling, no collective on the data path).
+device-output entry point (plato_pagerank_device) with the graph resident
+and no instrumentation; per-kernel times for the roofline come from a
+separate pass of the same steps.  `e2e` times the host-buffer C-ABI call
+plato_pagerank (ranks copied back to pinned host memory every step).  At
+N = 1 the same line carries `ppr_batch` (RMAT s22 seed 4, K = 64/256/1024
+queries per call against the plain one-query engine) and `serving` (RMAT s24
+seed 5, Poisson arrivals, p50/p99 latency).  Multi-GPU runs are independent
+replicas (weak scaling, no collective on the data path).
 
---impl reference times the CPU restatement of the reference engine (the
-oracle, C/OpenMP on all host threads) on the same graph: each step is one
-PageRank epoch (pull + vertex update) in the reference's double precision.
+--impl reference times the reference's CPU path on the host cores: the
+oracle's C/OpenMP restatement of the reference's pull PageRank, in the
+reference's double precision, one 20-epoch call per step on the same graph
+(built by the oracle's own RMAT generator, so no product code is loaded).
 """
 from __future__ import annotations
 
@@ -165,34 +171,51 @@ def cpu_pagerank_sample(V, src, dst, target_s=15.0):
     return E * n / dt / 1e9, n, dt, thr, E, ranks
 
 
+def bench_config(V: int, E: int, world: int) -> dict:
+    """The workload's config, identical in both arms."""
+    return {"workload": f"pagerank_rmat_s{SCALE}_ef{EDGEFACTOR}_seed{SEED}", "vertices": V, "edges": E,
+            "iterations": ITERATIONS, "damping": DAMPING, "parallelism": f"replicas{world}",
+            "step": f"one {ITERATIONS}-epoch PageRank call (pull), state buffers reused between calls",
+            "l2": "inputs larger than L2 (2.2 GB graph)"}
+
+
 def run_reference(args):
+    """The reference's CPU path on the host cores: the oracle's C/OpenMP
+    restatement of algo::pagerank (plato/algo/pagerank/pagerank.hpp:81-146)
+    on the same graph, one 20-epoch call per step with its rank buffers kept
+    between calls.  This process loads no product code: the graph comes from
+    the oracle's own RMAT generator (oracle/rmat.c), which the CPU tests hold
+    equal to the product's."""
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
     import oracle
-    import plato_b200 as pb
-    V, src, dst = pb.rmat(SCALE, EDGEFACTOR, SEED)
+    t0 = time.perf_counter()
+    V, src, dst = oracle.rmat(SCALE, EDGEFACTOR, SEED)
+    gen_s = time.perf_counter() - t0
     g = oracle.RefGraph(V, src, dst, True)
     E = g.stored_edges
     for _ in range(args.warmup):
-        g.pagerank(1, DAMPING, 0.0)
+        g.pagerank(ITERATIONS, DAMPING, 0.0)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        g.pagerank(1, DAMPING, 0.0)
+        g.pagerank(ITERATIONS, DAMPING, 0.0)
         times.append(time.perf_counter() - t0)
+    g.close()
     ms = float(np.mean(times)) * 1e3
-    val = E / (ms / 1e3) / 1e9
+    val = E * ITERATIONS / (ms / 1e3) / 1e9
     thr = oracle.max_threads()
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": "GTEPS", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"pagerank_rmat_s{SCALE}_ef{EDGEFACTOR}_seed{SEED}",
-                   "vertices": V, "edges": E, "step": "one PageRank epoch (pull + update)"},
+        "config": bench_config(V, E, world),
+        "setup": {"rmat_gen_s": gen_s, "generator": "oracle/rmat.c (equal to the product's, CPU tests)"},
         "cpu_baseline": {"value": val, "unit": "GTEPS", "cores": thr, "kind": "port",
-                         "sample": f"{args.steps} PageRank epochs of the s{SCALE} graph "
-                                   "(oracle ref_cpu.c, reference restatement, OpenMP)"},
+                         "sample": f"{args.steps} timed calls of {ITERATIONS} PageRank epochs on the "
+                                   f"whole s{SCALE} graph (oracle ref_cpu.c, the reference's pull "
+                                   "PageRank restated in C/OpenMP, FP64, host clock)"},
         "e2e": {"value": val, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -238,9 +261,8 @@ def run_plato(args):
         if dist:
             dist.barrier()
 
-    # ---- device-resident timed region --------------------------------------
-    lib.plato_profile_reset()
-    lib.plato_profile_enable(1)
+    # ---- device-resident timed region (no instrumentation) -------------------
+    lib.plato_profile_enable(0)
     launches0 = pb.kernel_launches()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -254,8 +276,18 @@ def run_plato(args):
         torch.cuda.synchronize()
     barrier()
     launches = pb.kernel_launches() - launches0
-    lib.plato_profile_enable(0)
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dist, "cuda")
+    value = world * E * ITERATIONS / (ms / 1e3) / 1e9
+
+    # ---- per-kernel device times: a separate pass of the same steps ----------
     import ctypes as C
+    prof_steps = max(1, min(args.steps, 5))
+    lib.plato_profile_reset()
+    lib.plato_profile_enable(1)
+    for _ in range(prof_steps):
+        step()
+    torch.cuda.synchronize()
+    lib.plato_profile_enable(0)
     kernel_times = {}
     for name in PULL_KERNELS:
         tot = C.c_double()
@@ -263,8 +295,6 @@ def run_plato(args):
         lib.plato_profile_read(name.encode(), C.byref(tot), C.byref(cnt))
         if cnt.value:
             kernel_times[name] = (tot.value, int(cnt.value))
-    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dist, "cuda")
-    value = world * E * ITERATIONS / (ms / 1e3) / 1e9
 
     # ---- end to end through the host-buffer C ABI ----------------------------
     host_out = torch.empty(V, dtype=torch.float32, pin_memory=True)
@@ -278,13 +308,10 @@ def run_plato(args):
     for _ in range(2):
         e2e_step()
     barrier()
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
     for _ in range(args.steps):
         e2e_step()
-    e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps, dist, "cuda")
     e2e_val = world * E * ITERATIONS / (e2e_ms / 1e3) / 1e9
@@ -293,7 +320,7 @@ def run_plato(args):
     peak, peak_kind = measured_peak()
     epoch_bytes = pr_algorithmic_bytes(V, E)
     bins = pull_bins(V, dst)
-    epochs = ITERATIONS * args.steps
+    epochs = ITERATIONS * prof_steps
     per = {}
     for name, (tot_ms, n) in kernel_times.items():
         per[name] = {"launches": n, "ms_per_launch": tot_ms / n}
@@ -315,28 +342,32 @@ def run_plato(args):
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": None, "kernel": dom,
-            "peak_source": f"{peak_kind} hbm_gbs (burst copy, of measured)",
+            "peak_source": f"{peak_kind} hbm_gbs (burst copy, of {peak_kind})",
             "bytes_per_launch": dom_bytes, "launch_ms": dom_ms,
+            "kernel_timing": f"CUDA events around each pull kernel on its launch stream, in a separate "
+                             f"pass of {prof_steps} steps right after the timed region",
             "pull_epoch": {"bytes": epoch_bytes, "ms": epoch_ms,
                            "achieved": epoch_bytes / (epoch_ms / 1e3) / 1e9 if epoch_ms else None,
-                           "frac": (epoch_bytes / (epoch_ms / 1e3) / 1e9 / peak) if epoch_ms else None},
+                           "frac": (epoch_bytes / (epoch_ms / 1e3) / 1e9 / peak) if epoch_ms else None,
+                           "step_frac": epoch_bytes * ITERATIONS / (ms / 1e3) / 1e9 / peak},
             "kernels": per, "bins": {"rows": bins["rows"], "edges": bins["edges"]}}
     prof = ROOT / "profiles" / f"{dom}_rmat_s{SCALE}_traffic.json"
     if prof.exists():
         tr = json.loads(prof.read_text())
         roof["traffic"] = tr.get("dram_bytes_per_launch")
+        roof["traffic_source"] = (f"profiles/{prof.name}: one ncu capture of this kernel on this workload, "
+                                  "not measured in this run")
 
     line = {
         "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"pagerank_rmat_s{SCALE}_ef{EDGEFACTOR}_seed{SEED}",
-                   "vertices": V, "edges": E, "iterations": ITERATIONS, "damping": DAMPING,
-                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (2.2 GB graph)",
-                   "graph_build_s": build_s, "rmat_gen_s": gen_s},
+        "config": bench_config(V, E, world),
+        "setup": {"graph_build_s": build_s, "rmat_gen_s": gen_s},
         "e2e": {"value": e2e_val, "unit": "GTEPS", "h2d_bytes_per_step": C.sizeof(opts),
                 "d2h_bytes_per_step": 4 * V, "ms_per_step": e2e_ms,
-                "note": "host-buffer plato_pagerank; graph resident in HBM"},
+                "note": "host-buffer plato_pagerank (ranks copied to pinned host memory every call; "
+                        "graph resident in HBM), host clock"},
         "gpu_launches": launches,
         "roofline": roof,
         "clocks": clk.summary(),
@@ -350,13 +381,92 @@ def run_plato(args):
         line["parity"] = {"vs": f"oracle ref_cpu.c FP64, {ITERATIONS} epochs, reference ranks / V",
                           "l1": float(err.sum()), "max_abs": float(err.max()), "tolerance_l1": 1e-6,
                           "ok": bool(err.sum() <= 1e-6)}
+    g.close()
+    del src, dst
+    if world == 1 and not args.no_extras:
+        # the metric's second half: batched PPR (s22 seed 4) and serving (s24 seed 5)
+        line["ppr_batch"] = bench_ppr_batch(pb)
+        line["serving"] = bench_serving(pb)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    g.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def bench_ppr_batch(pb, plain_n=16, reps=3):
+    """Batched multi-source PPR on RMAT s22 ef16 seed 4: K in 64/256/1024
+    queries per call, Zipf(1.5) seed sets of 1..32 vertices, eps 1e-6,
+    top-100 per query, against the plain engine (plato_seedset_ppr) answering
+    the same queries one at a time.  Host clock around whole calls, seed sets
+    from and top-k results to host memory."""
+    import oracle
+    t_all = time.perf_counter()
+    V, s, d = pb.rmat(22, 16, 4)
+    g = pb.Graph(V, s, d, is_directed=True)
+    deg = np.bincount(s, minlength=V)
+    sets = zipf_seed_sets(deg, 1024, 32, 4)
+    g.seedset_ppr(sets[0], 300, 0.85, 1e-6)
+    t0 = time.perf_counter()
+    plain = [g.seedset_ppr(sets[q], 300, 0.85, 1e-6)[0] for q in range(plain_n)]
+    plain_qps = plain_n / (time.perf_counter() - t0)
+    res = {"workload": "ppr_batch_rmat_s22_ef16_seed4", "vertices": V, "edges": int(s.size),
+           "unit": "queries/s", "eps": 1e-6, "topk": 100,
+           "plain_qps": plain_qps, "plain_sample": f"queries 0..{plain_n - 1}, one plato_seedset_ppr call each",
+           "timing": f"host clock around whole plato_ppr_batch calls (seed sets in, top-100 out), median of {reps}"}
+    for K in (64, 256, 1024):
+        g.ppr_batch(sets[:K], 300, 0.85, 1e-6, topk=100)  # autotune + warm
+        dts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            out = g.ppr_batch(sets[:K], 300, 0.85, 1e-6, topk=100)
+            dts.append(time.perf_counter() - t0)
+        dt = float(np.median(dts))
+        res[f"K{K}"] = {"qps": K / dt, "ms_per_batch": dt * 1e3, "speedup_vs_plain": K / dt / plain_qps,
+                        "iterations_max": int(out["iterations"].max()), "k_tile": g.ppr_batch_k_tile(K)}
+    # sampled columns: batch column vs the plain engine, and column 0 vs the FP64 oracle
+    chk = g.ppr_batch(sets[:plain_n], 300, 0.85, 1e-6, ranks=True)
+    res["l1_batch_vs_plain_max"] = max(float(np.abs(chk["ranks"][q].astype(np.float64) - plain[q]).sum())
+                                       for q in range(plain_n))
+    g.close()
+    ref = oracle.RefGraph(V, s, d, True)
+    want, ep, _ = ref.seedset_ppr(sets[0], 300, 0.85, 1e-6)
+    ref.close()
+    err = np.abs(chk["ranks"][0].astype(np.float64) - want)
+    res["parity_query0"] = {"vs": "oracle ref_cpu.c FP64", "l1": float(err.sum()), "max_abs": float(err.max()),
+                            "epochs": int(chk["iterations"][0]), "oracle_epochs": ep, "tolerance_l1": 1e-6,
+                            "ok": bool(err.sum() <= 1e-6)}
+    res["wall_s"] = time.perf_counter() - t_all
+    return res
+
+
+def bench_serving(pb, rates=(100, 1000, 5000, 20000), n_req=300, slots=256):
+    """PPR serving on RMAT s24 ef16 seed 5: Poisson arrivals at each offered
+    rate, Zipf(1.5) seed sets of 1..64, eps 1e-6, top-100; latency =
+    completion - arrival on the host clock; against the plain engine serving
+    one query at a time."""
+    t_all = time.perf_counter()
+    V, s, d = pb.rmat(24, 16, 5)
+    g = pb.Graph(V, s, d, is_directed=True)
+    deg = np.bincount(s, minlength=V)
+    del s, d
+    sets = zipf_seed_sets(deg, n_req, 64, 5)
+    g.seedset_ppr(sets[0], 300, 0.85, 1e-6)
+    t0 = time.perf_counter()
+    for q in range(8):
+        g.seedset_ppr(sets[q], 300, 0.85, 1e-6)
+    plain_qps = 8 / (time.perf_counter() - t0)
+    out = {"workload": "ppr_serving_rmat_s24_ef16_seed5", "vertices": V, "unit": "queries/s",
+           "slots": slots, "requests_per_rate": n_req, "plain_qps": plain_qps,
+           "timing": "host clock: latency = completion - arrival, sustained = requests / wall"}
+    out.update(_serve(pb, g, sets, rates, n_req, slots))
+    best = max(v["sustained_qps"] for k, v in out.items() if k.startswith("rate"))
+    out["best_sustained_qps"] = best
+    out["speedup_vs_plain"] = best / plain_qps
+    g.close()
+    out["wall_s"] = time.perf_counter() - t_all
+    return out
 
 
 def zipf_seed_sets(deg, K, max_size, seed):
@@ -713,6 +823,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["plato", "reference"], default="plato")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched-PPR and serving sections of the default line")
     ap.add_argument("--scale", type=int, default=SCALE,
                     help="RMAT scale (smaller values are for profiling captures only)")
     ap.add_argument("--suite", action="store_true",

@@ -9,7 +9,7 @@
  * [0, vertices) — the reference requires the same, see
  * plato/graph/structure/dcsc.hpp:48-49 "vertexId must be compacted" and
  * plato/graph/partition/sequence.hpp:67).  Internally the engine may renumber
- * vertices (PLATO_GRAPH_RELABEL); every result crosses the ABI in caller ids.
+ * vertices (unless PLATO_GRAPH_NO_RELABEL); every result crosses the ABI in caller ids.
  *
  * Numeric conventions (parity with the reference):
  *  - PageRank ranks are returned normalised: initial rank 1/V, teleport
@@ -39,14 +39,22 @@ extern "C" {
 #define PLATO_EINVAL      1  /* bad argument (null pointer, id out of range, ...) */
 #define PLATO_ENOMEM      2  /* device or host allocation failed / over budget     */
 #define PLATO_ECUDA       3  /* a CUDA runtime call failed                          */
-#define PLATO_ETIMEDOUT   4  /* a bounded device wait ran out                       */
+#define PLATO_ETIMEDOUT   4  /* reserved: no entry point of this version waits on the
+                                device for another agent, so none returns it        */
 #define PLATO_EBUSY       5  /* server full: no slot or HBM budget for the request  */
 #define PLATO_ENOTFOUND   6  /* nothing ready / unknown request id                  */
 
 #define PLATO_LEVEL_UNREACHED 0xFFFFFFFFu
 
-/* graph creation flags */
-#define PLATO_GRAPH_RELABEL 0x1u /* renumber vertices by descending in-degree inside the engine */
+/* graph creation flags.  By default the engine renumbers vertices by
+ * descending in-degree inside the graph (results still cross the ABI in
+ * caller ids): the pull kernels then work on contiguous degree bins.
+ * PLATO_GRAPH_NO_RELABEL keeps the caller's order (the device view's CSC is
+ * then indexed by caller ids); pull epochs on such a graph take the
+ * merge-path kernel, about 2.5x slower.  PLATO_GRAPH_RELABEL asks for the
+ * default explicitly; both together -> PLATO_EINVAL. */
+#define PLATO_GRAPH_RELABEL    0x1u
+#define PLATO_GRAPH_NO_RELABEL 0x2u
 
 /* personalized pagerank modes */
 #define PLATO_PPR_PULL      0 /* pull-only engine: personalized_pagerank.hpp:40-134     */
@@ -276,11 +284,18 @@ int plato_pagerank_device(plato_graph* g, const plato_pagerank_opts* opts, float
  * d_out_degree [V]; edges = directed edges stored, both directions for an
  * undirected graph), ranks written to device memory d_ranks [V] in the
  * caller's vertex order, normalised as plato_pagerank, on `stream`.
+ * d_ranks must be 16-byte aligned (it also holds the ranks between epochs
+ * and is read with vector loads), d_in_offsets 8-byte, d_in_adj and
+ * d_out_degree 4-byte aligned; otherwise PLATO_EINVAL before any launch.
  * Every temporary lives in one static device array of
  * PLATO_NOALLOC_SCRATCH_BYTES held by each GPU that loads the library until
  * exit; a graph needing more (about 4V + 12(V+E)/224 bytes) gets EINVAL.
  * The first call on a device looks up that array's device address (and sets
  * the kernel's shared-memory limit); make it before any stream capture.
+ * With eps > 0 the early exit is decided on the device; a non-NULL `stats`
+ * then makes the call wait for its own work at the end to read the epoch
+ * count and the last delta (stats->delta: the delta of the last non-final
+ * epoch, 0 with eps == 0, as plato_pagerank reports it).
  * Calls that overlap on the GPU race on the shared array: serialise them. */
 #define PLATO_NOALLOC_SCRATCH_BYTES (32u << 20)
 int plato_pagerank_csc_noalloc(uint32_t vertices, uint64_t edges, const uint64_t* d_in_offsets,

@@ -55,6 +55,10 @@ def load():
                                         P, P]
         lib.ref_bfs.argtypes = [P, C.c_uint32, C.c_double, P, P, P, P, P]
         lib.ref_max_threads.restype = C.c_int
+        lib.ref_rmat.argtypes = [C.c_uint32, C.c_uint32, C.c_uint64, C.c_double, C.c_double,
+                                 C.c_double, C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
+                                 C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.POINTER(C.c_uint32))]
+        lib.ref_rmat_free.argtypes = [P]
         _lib = lib
     return _lib
 
@@ -65,6 +69,26 @@ def _p(a: np.ndarray) -> C.c_void_p:
 
 def max_threads() -> int:
     return int(load().ref_max_threads())
+
+
+def rmat(scale: int, edgefactor: int, seed: int, symmetrize: bool = False,
+         a: float = 0.57, b: float = 0.19, c: float = 0.19):
+    """Seeded RMAT edge list (rmat.c, OpenMP) -> (V, src uint32, dst uint32),
+    sorted by (src, dst), self-loops and duplicates removed, ids compacted."""
+    lib = load()
+    V, n = C.c_uint32(), C.c_uint64()
+    ps, pd = C.POINTER(C.c_uint32)(), C.POINTER(C.c_uint32)()
+    r = lib.ref_rmat(scale, edgefactor, seed, a, b, c, 1 if symmetrize else 0, C.byref(V), C.byref(n),
+                     C.byref(ps), C.byref(pd))
+    if r != 0:
+        raise (ValueError if r == 1 else MemoryError)(f"ref_rmat failed ({r})")
+    try:
+        src = np.ctypeslib.as_array(ps, shape=(n.value,)).copy() if n.value else np.empty(0, np.uint32)
+        dst = np.ctypeslib.as_array(pd, shape=(n.value,)).copy() if n.value else np.empty(0, np.uint32)
+    finally:
+        lib.ref_rmat_free(C.cast(ps, C.c_void_p))
+        lib.ref_rmat_free(C.cast(pd, C.c_void_p))
+    return int(V.value), src, dst
 
 
 class RefGraph:

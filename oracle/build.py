@@ -1,6 +1,10 @@
-"""Build the oracle (test infrastructure): oracle/libref_cpu.so from ref_cpu.c.
+"""Build the oracle (test infrastructure): oracle/libref_cpu.so from ref_cpu.c
+and rmat.c, and, where the reference tree is present, oracle/_ref from the
+reference's own headers.
 
-    python -m oracle.build
+    python -m oracle.build [--force]
+
+The reference tree is found at $PLATO_REFERENCE_ROOT, else /root/reference.
 """
 from __future__ import annotations
 
@@ -10,22 +14,22 @@ import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-SRC = HERE / "ref_cpu.c"
+SRCS = [HERE / "ref_cpu.c", HERE / "rmat.c"]
 LIB = HERE / "libref_cpu.so"
 
 
 def build(force: bool = False) -> Path:
-    if not force and LIB.exists() and LIB.stat().st_mtime >= SRC.stat().st_mtime:
+    if not force and LIB.exists() and all(LIB.stat().st_mtime >= s.stat().st_mtime for s in SRCS):
         return LIB
     tmp = LIB.with_suffix(".so.tmp")
     cmd = ["gcc", "-O3", "-march=x86-64-v2", "-fopenmp", "-fPIC", "-shared", "-std=c11",
-           "-Wall", "-o", str(tmp), str(SRC), "-lm"]
+           "-Wall", "-o", str(tmp), *map(str, SRCS), "-lm"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
     return LIB
 
 
-REF_ROOT = Path("/root/reference")
+REF_ROOT = Path(os.environ.get("PLATO_REFERENCE_ROOT", "/root/reference"))
 REF_SHIM = HERE / "hll_ref_shim.cpp"
 REF_LIB = HERE / "_ref" / "libhll_ref.so"
 

@@ -57,6 +57,12 @@ typedef struct {
   uint32_t* out_adjs;     /* [E] */
   uint64_t stored_edges;
   uint32_t* out_degree;   /* from in-edges */
+  /* rank-loop state kept between calls (two V-vectors and two bitmaps), so a
+   * timed call is the epochs alone, like the device side's resident state */
+  double* ws_a;
+  double* ws_b;
+  uint64_t* ws_actives;
+  uint64_t* ws_walk;
 } ref_graph;
 
 /* ---------------- bitmap (bitmap.hpp) ------------------------------------ */
@@ -191,6 +197,10 @@ EXPORT void ref_graph_free(ref_graph* g) {
   free(g->row_index);
   free(g->out_adjs);
   free(g->out_degree);
+  free(g->ws_a);
+  free(g->ws_b);
+  free(g->ws_actives);
+  free(g->ws_walk);
   free(g);
 }
 
@@ -252,16 +262,23 @@ static inline double update(double* pval, double tele, double d, uint32_t deg, d
 /* Generic rank loop.  tele_kind selects pagerank / single-source / seed set.
  * pushpull: personalized_pagerank.hpp:158-272 push epochs while
  * active_edges <= edges/20 (sticky). */
-static int rank_loop(const ref_graph* g, int tele_kind, uint32_t src, const uint8_t* is_seed,
+static int rank_loop(ref_graph* g, int tele_kind, uint32_t src, const uint8_t* is_seed,
                      double seed_tele, uint32_t iteration, double damping, double eps,
                      int pushpull, double* out, uint32_t* epochs_out, uint32_t* push_epochs_out,
                      uint64_t* trace_out, double* delta_out) {
   const uint32_t V = g->vertices;
-  double* curt = (double*)malloc((size_t)V * 8);
-  double* next = (double*)malloc((size_t)V * 8);
-  uint64_t* actives = (uint64_t*)calloc(bm_words(V), 8);
-  uint64_t* walk = (uint64_t*)malloc(bm_words(V) * 8);
-  if (!curt || !next || !actives || !walk) return 2;
+  if (!g->ws_a) {
+    g->ws_a = (double*)malloc(((size_t)V + 1) * 8);
+    g->ws_b = (double*)malloc(((size_t)V + 1) * 8);
+    g->ws_actives = (uint64_t*)malloc(bm_words(V) * 8);
+    g->ws_walk = (uint64_t*)malloc(bm_words(V) * 8);
+    if (!g->ws_a || !g->ws_b || !g->ws_actives || !g->ws_walk) return 2;
+  }
+  double* curt = g->ws_a;
+  double* next = g->ws_b;
+  uint64_t* actives = g->ws_actives;
+  uint64_t* walk = g->ws_walk;
+  memset(actives, 0, bm_words(V) * 8);
   const uint32_t* odeg = g->out_degree;
   /* init */
 #pragma omp parallel for schedule(static)
@@ -348,22 +365,18 @@ static int rank_loop(const ref_graph* g, int tele_kind, uint32_t src, const uint
   if (push_epochs_out) *push_epochs_out = push_epochs;
   if (trace_out) *trace_out = trace;
   if (delta_out) *delta_out = delta;
-  free(curt);
-  free(next);
-  free(actives);
-  free(walk);
   return 0;
 }
 
 /* algo::pagerank — reference units (ranks start at 1.0). */
-EXPORT int ref_pagerank(const ref_graph* g, uint32_t iteration, double damping, double eps,
+EXPORT int ref_pagerank(ref_graph* g, uint32_t iteration, double damping, double eps,
                         double* out, uint32_t* epochs, double* delta) {
   return rank_loop(g, TELE_UNIFORM, 0, NULL, 0.0, iteration, damping, eps, 0, out, epochs, NULL,
                    NULL, delta);
 }
 
 /* algo::personalized_pagerank — pull-only (pushpull = 0) or dual-mode (1). */
-EXPORT int ref_ppr(const ref_graph* g, uint32_t src, uint32_t iteration, double damping, double eps,
+EXPORT int ref_ppr(ref_graph* g, uint32_t src, uint32_t iteration, double damping, double eps,
                    int pushpull, double* out, uint32_t* epochs, uint32_t* push_epochs,
                    uint64_t* trace, double* delta) {
   if (src >= g->vertices) return 1;
@@ -373,7 +386,7 @@ EXPORT int ref_ppr(const ref_graph* g, uint32_t src, uint32_t iteration, double 
 
 /* Seed-set PPR with trustrank's semantics (trustrank.hpp:197-245): init
  * 1/|S| on seeds (divided by degree), teleport (1-d)/|S| on seeds. */
-EXPORT int ref_seedset_ppr(const ref_graph* g, uint32_t nseeds, const uint32_t* seeds,
+EXPORT int ref_seedset_ppr(ref_graph* g, uint32_t nseeds, const uint32_t* seeds,
                            uint32_t iteration, double damping, double eps, double* out,
                            uint32_t* epochs, double* delta) {
   const uint32_t V = g->vertices;

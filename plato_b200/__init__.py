@@ -25,7 +25,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from ._lib import (PLATO_GRAPH_RELABEL, PLATO_LEVEL_UNREACHED, PLATO_PPR_PULL, PLATO_PPR_PUSHPULL,
+from ._lib import (PLATO_GRAPH_NO_RELABEL, PLATO_GRAPH_RELABEL, PLATO_LEVEL_UNREACHED, PLATO_PPR_PULL, PLATO_PPR_PUSHPULL,
                    PlatoError, check, load)
 
 __all__ = [
@@ -183,7 +183,7 @@ class Graph:
         info = _lib.GraphInfo(1 if is_directed else 0, int(vertices), int(src.size),
                               max(int(vertices) - 1, 0))
         h = C.c_void_p()
-        flags = PLATO_GRAPH_RELABEL if relabel else 0
+        flags = PLATO_GRAPH_RELABEL if relabel else PLATO_GRAPH_NO_RELABEL
         if weights is None:
             check(self._lib.plato_graph_create(C.byref(info), _ptr(src), _ptr(dst), flags, C.byref(h)),
                   "plato_graph_create")

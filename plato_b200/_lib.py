@@ -14,7 +14,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libplato_b200.so"
 PLATO_OK, PLATO_EINVAL, PLATO_ENOMEM, PLATO_ECUDA, PLATO_ETIMEDOUT, PLATO_EBUSY, PLATO_ENOTFOUND = range(7)
 PLATO_VALUE_F32, PLATO_VALUE_U32 = 0, 1  # plato_write_vertex_csv value types
 PLATO_LEVEL_UNREACHED = 0xFFFFFFFF
-PLATO_GRAPH_RELABEL = 0x1
+PLATO_GRAPH_RELABEL, PLATO_GRAPH_NO_RELABEL = 0x1, 0x2
 PLATO_PPR_PULL, PLATO_PPR_PUSHPULL = 0, 1
 
 STATUS_NAMES = {0: "PLATO_OK", 1: "PLATO_EINVAL", 2: "PLATO_ENOMEM", 3: "PLATO_ECUDA",

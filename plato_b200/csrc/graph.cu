@@ -9,7 +9,7 @@
 // (dcsc.hpp:365-385).  Out-degrees are counted from the in-edge structure, as
 // generate_dense_out_degrees_fg does (structure.hpp:291-346).
 //
-// With PLATO_GRAPH_RELABEL the engine renumbers vertices by descending
+// By default (unless PLATO_GRAPH_NO_RELABEL) the engine renumbers vertices by descending
 // in-degree (ties by caller id): CSC columns then form contiguous degree
 // bins for the pull kernels, and since in- and out-degree go together in
 // power-law graphs the most-gathered rank values share cache lines at the
@@ -319,7 +319,7 @@ int create_impl(const plato_graph_info* info, const uint32_t* src, const uint32_
                                        " edges have an endpoint >= vertices (ids must be compact)");
 
   dbuf<uint8_t> tmp;
-  g->relabeled = (flags & PLATO_GRAPH_RELABEL) != 0 && V > 1;
+  g->relabeled = (flags & PLATO_GRAPH_NO_RELABEL) == 0 && V > 1;
   if (g->relabeled) {
     dbuf<uint64_t> ka, kb;
     PLATO_TRY(ka.alloc(V));
@@ -457,6 +457,10 @@ int create_checked(const plato_graph_info* info, const plato_vid_t* src, const p
   if (info->edges > 0 && (!src || !dst))
     return set_error(PLATO_EINVAL, std::string(who) + ": null edge arrays");
   if (info->vertices == 0) return set_error(PLATO_EINVAL, std::string(who) + ": zero vertices");
+  if ((flags & PLATO_GRAPH_RELABEL) && (flags & PLATO_GRAPH_NO_RELABEL))
+    return set_error(PLATO_EINVAL, std::string(who) + ": PLATO_GRAPH_RELABEL and PLATO_GRAPH_NO_RELABEL together");
+  if (flags & ~(PLATO_GRAPH_RELABEL | PLATO_GRAPH_NO_RELABEL))
+    return set_error(PLATO_EINVAL, std::string(who) + ": unknown flag bits");
   plato_graph* g = new (std::nothrow) plato_graph();
   if (!g) return set_error(PLATO_ENOMEM, std::string(who) + ": host allocation failed");
   const int s = create_impl(info, src, dst, weights, flags, g);

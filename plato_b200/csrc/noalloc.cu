@@ -13,11 +13,19 @@
 // The array (kNoAllocScratchBytes) is held by every GPU that loads the
 // library until the process exits.  All calls share it and it keeps the
 // previous call's contents; everything a call reads from it is written by
-// the same call first, so no clearing is needed.  Calls whose work overlaps
-// on the GPU (two streams, two host threads) race on it: serialise them.
+// the same call first (the epoch-control words by a launch at the start of
+// the call), so no clearing is needed.  Calls whose work overlaps on the GPU
+// (two streams, two host threads) race on it: serialise them.
+//
+// With eps > 0 the early exit of pagerank.hpp:137-139 is decided on the
+// device (k_epoch_control after each epoch, as the main path does): every
+// epoch is enqueued, those after the last one return at once, and a last
+// launch moves the result into d_ranks when it ended in the scratch buffer.
+#include <cstdint>
 #include <mutex>
 
 #include "common.cuh"
+#include "pull_binned.cuh"
 #include "pull_merge.cuh"
 #include "pull_warp.cuh"
 
@@ -92,7 +100,26 @@ __global__ void k_na_init(const uint32_t* __restrict__ deg, uint32_t V, float* x
   }
 }
 
+// ctrl = {epoch kind (0 normal, 1 final, 2 done), epochs run}; see k_epoch_control.
+__global__ void k_na_ctrl_init(int* ctrl, uint32_t iteration, double* delta) {
+  ctrl[0] = iteration == 1 ? 1 : 0;
+  ctrl[1] = 0;
+  delta[0] = 0.0;
+}
+
+// After the epochs of an eps > 0 call: the state ended in buf[ran & 1]; copy
+// it to d_ranks (buf[0]) when it is the scratch buffer.
+__global__ void k_na_finish(const int* __restrict__ ctrl, const float* __restrict__ x2,
+                            float* __restrict__ out, uint32_t V) {
+  if ((ctrl[1] & 1) == 0) return;
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+       v += (uint64_t)gridDim.x * blockDim.x)
+    out[v] = x2[v];
+}
+
 size_t align256(size_t n) { return (n + 255) / 256 * 256; }
+
+bool aligned(const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; }
 
 }  // namespace
 }  // namespace plato_b200
@@ -110,6 +137,13 @@ extern "C" int plato_pagerank_csc_noalloc(uint32_t vertices, uint64_t edges,
   if (opts->iteration == 0) return set_error(PLATO_EINVAL, "iteration must be >= 1");
   if (!(opts->damping >= 0.0 && opts->damping <= 1.0))
     return set_error(PLATO_EINVAL, "damping must be in [0, 1]");
+  // d_ranks doubles as the first state buffer, which the pull kernel reads
+  // with 16-byte vector loads; the other arrays need their natural alignment.
+  if (!aligned(d_ranks, 16) || !aligned(d_in_offsets, 8) || !aligned(d_out_degree, 4) ||
+      (d_in_adj && !aligned(d_in_adj, 4)))
+    return set_error(PLATO_EINVAL,
+                     "plato_pagerank_csc_noalloc: d_ranks must be 16-byte aligned, d_in_offsets "
+                     "8-byte aligned, d_in_adj and d_out_degree 4-byte aligned");
   int dev = 0;
   PLATO_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return set_error(PLATO_EINVAL, "device index out of range");
@@ -117,11 +151,14 @@ extern "C" int plato_pagerank_csc_noalloc(uint32_t vertices, uint64_t edges,
   const uint32_t sms = g_sms[dev];
   const uint32_t Wr = sms * na_cfg::kWarps;
   const uint64_t W = Wr;
-  // scratch layout: x2 [V] | trow [T+1] | tedge [T+1] | carry [W] | head [W] | partials, delta
+  const uint32_t fix_blocks = (Wr + 255) / 256;
+  const uint32_t nparts = sms + fix_blocks;
+  // scratch layout: x2 [V] | trow [T+1] | tedge [T+1] | carry [W] | head [W] |
+  //                 partials [nparts] + delta | ctrl [2]
   const uint64_t items = na_cfg::kItems;
   const uint64_t T = (static_cast<uint64_t>(vertices) + edges + items - 1) / items;
   const size_t need = align256(4ull * vertices) + align256(4ull * (T + 1)) + align256(8ull * (T + 1)) +
-                      2 * align256(4ull * W) + align256(8ull * (sms + (W + 255) / 256 + 1));
+                      2 * align256(4ull * W) + align256(8ull * (nparts + 1)) + align256(2 * sizeof(int));
   if (need > kNoAllocScratchBytes || T >= 0xFFFFFFFFull)
     return set_error(PLATO_EINVAL,
                      "plato_pagerank_csc_noalloc: graph needs " + std::to_string(need) +
@@ -141,8 +178,9 @@ extern "C" int plato_pagerank_csc_noalloc(uint32_t vertices, uint64_t edges,
   float* head = reinterpret_cast<float*>(base + o);
   o += align256(4ull * W);
   double* partials = reinterpret_cast<double*>(base + o);
-  const uint32_t fix_blocks = (Wr + 255) / 256;
-  double* delta_dev = partials + sms + fix_blocks;
+  double* delta_dev = partials + nparts;
+  o += align256(8ull * (nparts + 1));
+  int* ctrl = reinterpret_cast<int*>(base + o);
 
   k_na_merge_tiles<<<grid_for(T + 1, 256), 256, 0, st>>>(d_in_offsets, vertices, edges,
                                                          static_cast<uint32_t>(items),
@@ -154,12 +192,16 @@ extern "C" int plato_pagerank_csc_noalloc(uint32_t vertices, uint64_t edges,
   const float d = static_cast<float>(opts->damping);
   const teleport_uniform tele{static_cast<float>((1.0 - opts->damping) / vertices)};
   const uint32_t H = std::min<uint32_t>(vertices, g_hub_cap[dev]);
+  const bool device_exit = opts->eps > 0.0;
+  if (device_exit) {
+    k_na_ctrl_init<<<1, 1, 0, st>>>(ctrl, opts->iteration, delta_dev);
+    PLATO_LAUNCHED("k_na_ctrl_init");
+  }
   int cur = 0;
-  uint32_t epochs = 0;
-  double delta = 0.0;
   for (uint32_t epoch = 0; epoch < opts->iteration; ++epoch) {
-    const bool final_epoch = (epoch == opts->iteration - 1);
-    na_update upd{buf[cur], buf[cur ^ 1], d_out_degree, tele, d, final_epoch ? 1 : 0};
+    const bool final_epoch = !device_exit && (epoch == opts->iteration - 1);
+    na_update upd{buf[cur], buf[cur ^ 1], d_out_degree, tele, d, final_epoch ? 1 : 0,
+                  device_exit ? ctrl : nullptr};
     pull_warp_args a{trow, tedge, static_cast<uint32_t>(T), edges, d_in_offsets, d_in_adj,
                      buf[cur], H, carry, head, partials};
     k_pull_warp<kNoAllocIPT, na_update><<<sms, 1024, na_cfg::smem_bytes(H), st>>>(a, upd);
@@ -167,21 +209,31 @@ extern "C" int plato_pagerank_csc_noalloc(uint32_t vertices, uint64_t edges,
     a.partials = partials + sms;
     k_pull_warp_fixup<na_update><<<fix_blocks, 256, 0, st>>>(a, Wr, upd);
     PLATO_LAUNCHED("k_pull_warp_fixup (no-alloc)");
-    ++epochs;
-    if (!final_epoch && opts->eps > 0.0) {
-      k_sum_partials<<<1, 1024, 0, st>>>(partials, sms + fix_blocks, delta_dev);
-      PLATO_LAUNCHED("k_sum_partials (no-alloc)");
-      PLATO_CUDA_TRY(cudaMemcpyAsync(&delta, delta_dev, sizeof(double), cudaMemcpyDeviceToHost, st));
-      PLATO_CUDA_TRY(cudaStreamSynchronize(st));
-      delta *= static_cast<double>(vertices);
-      if (delta < opts->eps) epoch = opts->iteration - 2;
+    if (device_exit) {
+      // delta in the reference's units (its ranks sum to ~V)
+      k_epoch_control<<<1, 1024, 0, st>>>(partials, nparts, ctrl, delta_dev,
+                                          static_cast<double>(vertices), opts->eps, opts->iteration);
+      PLATO_LAUNCHED("k_epoch_control (no-alloc)");
     }
     cur ^= 1;
   }
-  if (buf[cur] != d_ranks)
+  if (device_exit) {
+    k_na_finish<<<grid_for(vertices, 256), 256, 0, st>>>(ctrl, x2, d_ranks, vertices);
+    PLATO_LAUNCHED("k_na_finish");
+  } else if (buf[cur] != d_ranks) {
     PLATO_CUDA_TRY(cudaMemcpyAsync(d_ranks, buf[cur], 4ull * vertices, cudaMemcpyDeviceToDevice, st));
+  }
   if (stats) {
     *stats = plato_run_stats{};
+    uint32_t epochs = opts->iteration;
+    double delta = 0.0;
+    if (device_exit) {  // the epoch count and last delta are on the device: wait for them
+      int h_ctrl[2] = {0, 0};
+      PLATO_CUDA_TRY(cudaMemcpyAsync(h_ctrl, ctrl, sizeof(h_ctrl), cudaMemcpyDeviceToHost, st));
+      PLATO_CUDA_TRY(cudaMemcpyAsync(&delta, delta_dev, sizeof(double), cudaMemcpyDeviceToHost, st));
+      PLATO_CUDA_TRY(cudaStreamSynchronize(st));
+      epochs = static_cast<uint32_t>(h_ctrl[1]);
+    }
     stats->iterations = epochs;
     stats->pull_iterations = epochs;
     stats->delta = delta;

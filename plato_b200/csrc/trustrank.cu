@@ -42,10 +42,14 @@ __global__ void k_tr_init(double* x, const uint32_t* __restrict__ deg, uint32_t 
 }
 
 // pagerank.hpp:118-135: r = (1-d) + d*y; non-final epochs divide by the degree
-// and sum |x' - x| * deg into *delta.  The epoch is final when it is the last
-// one or when ctrl[1] says so; nothing runs once ctrl[0] is set.
-__global__ void k_tr_update(double* n, const double* __restrict__ c, const uint32_t* __restrict__ deg,
-                            uint32_t V, double d, int last_epoch, double* delta, const uint32_t* ctrl) {
+// and sum |x' - x| * deg, one partial per block (summed in a fixed order by
+// k_tr_control, so the exit epoch does not depend on atomic order).  The
+// epoch is final when it is the last one or when ctrl[1] says so; nothing
+// runs once ctrl[0] is set.
+__global__ void __launch_bounds__(256) k_tr_update(double* n, const double* __restrict__ c,
+                                                   const uint32_t* __restrict__ deg, uint32_t V, double d,
+                                                   int last_epoch, double* partials, const uint32_t* ctrl) {
+  __shared__ double s_red[32];
   if (ctrl[0]) return;
   const bool last = last_epoch || ctrl[1];
   double dl = 0.0;
@@ -62,8 +66,8 @@ __global__ void k_tr_update(double* n, const double* __restrict__ c, const uint3
     }
     n[v] = r;
   }
-  dl = warp_sum(dl);
-  if ((threadIdx.x & 31) == 0 && dl != 0.0) atomicAdd(delta, dl);
+  dl = block_sum<256>(dl, s_red);
+  if (threadIdx.x == 0) partials[blockIdx.x] = dl;
 }
 
 // next.fill(0) of the epoch, skipped like the rest once the final epoch has
@@ -76,18 +80,27 @@ __global__ void k_tr_zero(double* n, uint32_t V, const uint32_t* ctrl) {
 }
 
 // The eps early exit of pagerank.hpp:137-139 decided on the device, so the
-// host enqueues every epoch without waiting: after a non-final epoch with
-// delta < eps the next epoch is the final one (ctrl[1]); after the final
-// epoch ctrl[0] stops the rest and ctrl[2] records which epoch it was.
-__global__ void k_tr_control(double* delta, double eps, uint32_t epoch, int last_epoch, uint32_t* ctrl) {
-  if (ctrl[0]) return;
+// host enqueues every epoch without waiting: the epoch's delta is the sum of
+// the update's n block partials in a fixed order; after a non-final epoch
+// with delta < eps the next epoch is the final one (ctrl[1]); after the
+// final epoch ctrl[0] stops the rest and ctrl[2] records which epoch it was.
+__global__ void __launch_bounds__(1024) k_tr_control(const double* __restrict__ partials, uint32_t n,
+                                                     double eps, uint32_t epoch, int last_epoch,
+                                                     uint32_t* ctrl) {
+  __shared__ double s_red[32];
+  if (ctrl[0]) return;  // grid-uniform
+  const uint32_t per = (n + 1023) / 1024;
+  const uint32_t b = threadIdx.x * per, e = min(n, b + per);
+  double s = 0.0;
+  for (uint32_t i = b; i < e; ++i) s += partials[i];
+  s = block_sum<1024>(s, s_red);
+  if (threadIdx.x != 0) return;
   if (last_epoch || ctrl[1]) {
     ctrl[0] = 1;
     ctrl[2] = epoch;
-  } else if (*delta < eps) {
+  } else if (s < eps) {
     ctrl[1] = 1;
   }
-  *delta = 0.0;
 }
 
 // Selection ranks laid out by caller id, with the caller ids beside them.
@@ -155,15 +168,15 @@ std::vector<uint32_t> selection_top(plato_graph* g, bool inverse, uint32_t k) {
   const uint32_t* deg = inverse ? view.in_degree : view.out_degree;
   const uint32_t V = engine.vertices();
   dense_state_t<double> x[2] = {engine.alloc_v_state<double>(), engine.alloc_v_state<double>()};
-  double* delta = nullptr;
+  double* delta = nullptr;  // the update's block partials
   uint32_t* ctrl = nullptr;
   int* unused = nullptr;
-  dev_alloc(&delta, sizeof(double), "trustrank delta");
+  const unsigned upd_blocks = grid_for(V, 256);
+  dev_alloc(&delta, upd_blocks * sizeof(double), "trustrank delta");
   uint32_t final_epoch = 0;
   try {
     dev_alloc(&ctrl, 3 * sizeof(uint32_t), "trustrank control");
     dev_alloc(&unused, sizeof(int), "trustrank slot sum");
-    check_cuda(cudaMemset(delta, 0, sizeof(double)), "trustrank delta");
     check_cuda(cudaMemset(ctrl, 0, 3 * sizeof(uint32_t)), "trustrank control");
     k_tr_init<<<grid_for(V, 256), 256>>>(x[0].data(), deg, V);
     check_cuda(cudaGetLastError(), "k_tr_init");
@@ -187,9 +200,9 @@ std::vector<uint32_t> selection_top(plato_graph* g, bool inverse, uint32_t k) {
           },
           unused);
       const int last = epoch + 1 == kIterations ? 1 : 0;
-      k_tr_update<<<grid_for(V, 256), 256>>>(n, c, deg, V, kDamping, last, delta, ctrl);
+      k_tr_update<<<upd_blocks, 256>>>(n, c, deg, V, kDamping, last, delta, ctrl);
       check_cuda(cudaGetLastError(), "k_tr_update");
-      k_tr_control<<<1, 1>>>(delta, kEps, epoch, last, ctrl);
+      k_tr_control<<<1, 1024>>>(delta, upd_blocks, kEps, epoch, last, ctrl);
       check_cuda(cudaGetLastError(), "k_tr_control");
       count_launch(5);
     }

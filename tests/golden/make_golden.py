@@ -18,6 +18,7 @@ The reference tree is only needed to regenerate; tests read the outputs.
 from __future__ import annotations
 
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -150,4 +151,5 @@ def main(root: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    main(Path(sys.argv[1]) if len(sys.argv) > 1 else
+         Path(os.environ.get("PLATO_REFERENCE_ROOT", "/root/reference")))

@@ -61,3 +61,27 @@ def test_version():
 def test_missing_library_fails_loudly(tmp_path):
     with pytest.raises(ImportError):
         _lib.load(tmp_path / "nope.so")
+
+
+def test_graph_flags_checked_before_any_device_work():
+    lib = _lib.load()
+    info = _lib.GraphInfo(1, 3, 0, 2)
+    h = C.c_void_p()
+    both = _lib.PLATO_GRAPH_RELABEL | _lib.PLATO_GRAPH_NO_RELABEL
+    assert lib.plato_graph_create(C.byref(info), None, None, both, C.byref(h)) == _lib.PLATO_EINVAL
+    assert lib.plato_graph_create(C.byref(info), None, None, 0x80, C.byref(h)) == _lib.PLATO_EINVAL
+
+
+def test_noalloc_rejects_unaligned_buffers_before_any_device_work():
+    """The alignment rules of plato_pagerank_csc_noalloc are checked on the
+    host before any CUDA call, so a bad pointer gives PLATO_EINVAL (not a
+    device fault) even here, with no GPU and pointers that are never touched."""
+    lib = _lib.load()
+    o = _lib.PagerankOpts(5, 0.85, 0.0)
+    good = 1 << 20
+    for ranks, off, adj, deg in ((good + 4, good, good, good), (good, good + 4, good, good),
+                                 (good, good, good + 2, good), (good, good, good, good + 1)):
+        rc = lib.plato_pagerank_csc_noalloc(3, 2, C.c_void_p(off), C.c_void_p(adj), C.c_void_p(deg),
+                                            C.byref(o), C.c_void_p(ranks), None, None)
+        assert rc == _lib.PLATO_EINVAL
+        assert b"aligned" in lib.plato_last_error()

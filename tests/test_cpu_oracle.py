@@ -69,6 +69,42 @@ def test_rmat_generator_matches_spec(scale, sym, perm):
     assert ids.size == V and ids[0] == 0 and ids[-1] == V - 1  # compact
 
 
+@pytest.mark.parametrize("scale,sym", [(6, False), (11, True), (16, False)])
+def test_oracle_rmat_matches_product_and_spec(scale, sym):
+    """bench.py's reference arm generates its graph with the oracle's C
+    generator (so that its process never loads the product library); the
+    lists must equal the product's and the numpy restatement's."""
+    import oracle
+    import plato_b200 as pb
+    V, s, d = oracle.rmat(scale, 16, 3, symmetrize=sym)
+    V1, s1, d1 = pb.rmat(scale, 16, 3, symmetrize=sym)
+    assert V == V1
+    np.testing.assert_array_equal(s, s1)
+    np.testing.assert_array_equal(d, d1)
+    if scale <= 11:
+        V2, s2, d2 = rmat_spec.rmat(scale, 16, 3, symmetrize=sym)
+        assert V == V2
+        np.testing.assert_array_equal(s, s2)
+        np.testing.assert_array_equal(d, d2)
+
+
+def test_oracle_rank_state_reused_between_calls():
+    """The oracle keeps its rank-loop buffers on the graph between calls; a
+    second call (and a call of another kind in between) gives the same bits."""
+    import oracle
+    V, s, d = oracle.rmat(10, 16, 5)
+    g = oracle.RefGraph(V, s, d, True)
+    try:
+        a, ea, _ = g.pagerank(20, 0.85, 0.0)
+        src = int(np.flatnonzero(g.out_degrees() > 0)[0])
+        g.ppr(src, 30, 0.85, 0.0, True)
+        b, eb, _ = g.pagerank(20, 0.85, 0.0)
+    finally:
+        g.close()
+    assert ea == eb == 20
+    np.testing.assert_array_equal(a, b)
+
+
 @pytest.mark.parametrize("directed", [True, False])
 def test_oracle_pagerank_vs_fp64(directed):
     import plato_b200 as pb

@@ -3,7 +3,8 @@ C/OpenMP restatement (oracle/ref_cpu.c) on the same inputs:
 
 * BFS, RMAT scale 22 ef 16 seed 2 symmetrised (the 64-root traversal
   workload): levels bit-exact, visited count, epoch count and push/pull trace
-  equal, for 3 of the same roots; parents one level up along real edges.
+  equal, for all 64 of the same roots; parents one level up along real edges
+  (checked against the sorted edge set for the first 3 roots).
 * PageRank, RMAT scale 24 ef 16 seed 3, 20 pull epochs: L1 <= 1e-6 against
   the reference's ranks / V.
 * Single-source PPR on the same graph to delta < 1e-7, pull and push-pull:
@@ -55,20 +56,22 @@ def pr_graph():
 def test_bfs_s22_levels_bit_exact(bfs_graph):
     V, s, d, ref, g = bfs_graph
     deg = np.bincount(s, minlength=V) + np.bincount(d, minlength=V)
-    roots = np.random.default_rng(2).choice(np.flatnonzero(deg > 0), 64, replace=False)[:3]
+    roots = np.random.default_rng(2).choice(np.flatnonzero(deg > 0), 64, replace=False)
     ek = np.sort(np.concatenate([(s.astype(np.uint64) << np.uint64(32)) | d.astype(np.uint64),
                                  (d.astype(np.uint64) << np.uint64(32)) | s.astype(np.uint64)]))
-    for root in roots:
+    for i, root in enumerate(roots):
         lev_ref, _, vis_ref, tr_ref, ep_ref = ref.bfs(int(root), 0.05)
         lev, par, st = g.bfs(int(root))
         np.testing.assert_array_equal(lev, lev_ref)
         assert st.visited == vis_ref
         assert st.iterations == ep_ref
-        trace = [bool((tr_ref >> i) & 1) for i in range(min(ep_ref, 64))]
+        trace = [bool((tr_ref >> k) & 1) for k in range(min(ep_ref, 64))]
         assert [m == "push" for m in st.mode_trace] == trace
         reached = np.flatnonzero((lev != pb.PLATO_LEVEL_UNREACHED) & (np.arange(V) != root))
         assert par[root] == root
         assert (lev[par[reached]] == lev[reached] - 1).all()
+        if i >= 3:
+            continue
         key = (par[reached].astype(np.uint64) << np.uint64(32)) | reached.astype(np.uint64)
         pos = np.minimum(np.searchsorted(ek, key), ek.size - 1)
         assert (ek[pos] == key).all()  # every parent link is an edge
