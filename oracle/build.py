@@ -32,23 +32,47 @@ def build(force: bool = False) -> Path:
 REF_ROOT = Path(os.environ.get("PLATO_REFERENCE_ROOT", "/root/reference"))
 REF_SHIM = HERE / "hll_ref_shim.cpp"
 REF_LIB = HERE / "_ref" / "libhll_ref.so"
+PLATO_SHIM = HERE / "ref_shim" / "plato_ref_shim.cpp"
+PLATO_SHIM_INC = HERE / "ref_shim" / "include"
+PLATO_LIB = HERE / "_ref" / "libplato_ref.so"
+
+
+def _newer(lib: Path, *deps: Path) -> bool:
+    return lib.exists() and all(lib.stat().st_mtime >= d.stat().st_mtime for d in deps)
 
 
 def build_ref(force: bool = False, ref_root: Path = REF_ROOT) -> Path | None:
-    """Compile oracle/_ref/libhll_ref.so: hll_ref_shim.cpp over the reference's
-    own plato/util/hyperloglog.hpp + hash.hpp, read where they lie in the
-    reference tree (header-only, no dependencies).  Returns None when the
-    reference tree is absent (the committed golden vectors stand in)."""
+    """Compile the reference's own code into oracle/_ref, from its sources
+    where they lie in the reference tree:
+      libhll_ref.so    hll_ref_shim.cpp over plato/util/hyperloglog.hpp +
+                       hash.hpp (header-only, no dependencies);
+      libplato_ref.so  ref_shim/plato_ref_shim.cpp over the engine, graph and
+                       algorithm headers (pagerank, personalized_pagerank, bfs,
+                       trustrank), against the one-rank stand-ins in
+                       ref_shim/include for the libraries the reference needs.
+    Returns None when the reference tree is absent (the committed golden
+    vectors under tests/golden/ stand in)."""
     if not (ref_root / "plato" / "util" / "hyperloglog.hpp").exists():
         return None
-    if not force and REF_LIB.exists() and REF_LIB.stat().st_mtime >= REF_SHIM.stat().st_mtime:
-        return REF_LIB
     REF_LIB.parent.mkdir(exist_ok=True)
-    tmp = REF_LIB.with_suffix(".so.tmp")
-    cmd = ["g++", "-O2", "-fPIC", "-shared", "-std=c++14", "-I", str(ref_root), "-o", str(tmp),
-           str(REF_SHIM)]
-    subprocess.run(cmd, check=True)
-    os.replace(tmp, REF_LIB)
+    if force or not _newer(REF_LIB, REF_SHIM):
+        tmp = REF_LIB.with_suffix(".so.tmp")
+        cmd = ["g++", "-O2", "-fPIC", "-shared", "-std=c++14", "-I", str(ref_root), "-o", str(tmp),
+               str(REF_SHIM)]
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, REF_LIB)
+    if (ref_root / "plato" / "engine" / "dualmode.hpp").exists():
+        stubs = [p for p in PLATO_SHIM_INC.rglob("*") if p.is_file()]
+        if force or not _newer(PLATO_LIB, PLATO_SHIM, *stubs):
+            tmp = PLATO_LIB.with_suffix(".so.tmp")
+            # the stand-ins come first on the include path; __DUALMODE_DEBUG__
+            # makes the engine log its push/pull choice (dualmode.hpp:281-293)
+            cmd = ["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-w", "-D__DUALMODE_DEBUG__",
+                   "-I", str(PLATO_SHIM_INC), "-I", str(ref_root),
+                   "-I", str(ref_root / "plato" / "util" / "libcuckoo"),
+                   "-o", str(tmp), str(PLATO_SHIM), "-Wl,--no-undefined"]
+            subprocess.run(cmd, check=True)
+            os.replace(tmp, PLATO_LIB)
     return REF_LIB
 
 

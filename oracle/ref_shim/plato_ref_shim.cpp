@@ -36,6 +36,7 @@
 #include "plato/algo/pagerank/pagerank.hpp"
 #include "plato/algo/ppr/personalized_pagerank.hpp"
 #include "plato/algo/bfs/bfs.hpp"
+#include "plato/algo/trustrank/trustrank.hpp"
 
 DEFINE_int32(threads, -1, "threads (the reference's --threads)");
 
@@ -184,6 +185,13 @@ __attribute__((visibility("default"))) void* refp_graph_build(uint32_t vertices,
 
 __attribute__((visibility("default"))) void refp_graph_free(void* h) { delete static_cast<ref_graph*>(h); }
 
+// Threads the reference runs its OpenMP loops on (cluster_info_t::threads_,
+// from --threads, OMP_NUM_THREADS or every configured CPU, base.hpp:194-202).
+__attribute__((visibility("default"))) int refp_threads(void) {
+  init_once();
+  return plato::cluster_info_t::get_instance().threads_;
+}
+
 // graph_info_t of the built graph: {vertices, max_v_i, edges}
 __attribute__((visibility("default"))) void refp_graph_info(void* h, uint32_t* vertices, uint32_t* max_v_i,
                                                             uint64_t* edges) {
@@ -212,11 +220,10 @@ __attribute__((visibility("default"))) int refp_pagerank(void* h, uint32_t itera
 }
 
 // algo::personalized_pagerank: pull-only (personalized_pagerank.hpp:40-134)
-// or dual-mode (:137-275) when pushpull != 0.  *trace: bit i = epoch i ran
-// push-mode (dual-mode only; from the engine's debug lines).
+// or dual-mode (:137-275) when pushpull != 0.  Ranks [max_v_i + 1];
+// *epochs = epochs logged.
 __attribute__((visibility("default"))) int refp_ppr(void* h, uint32_t src, uint32_t iteration, double damping,
-                                                    double eps, int pushpull, double* out, uint32_t* epochs,
-                                                    uint64_t* trace) {
+                                                    double eps, int pushpull, double* out, uint32_t* epochs) {
   auto* g = static_cast<ref_graph*>(h);
   plato::algo::personalized_pagerank_opts_t opts;
   opts.iteration_ = iteration;
@@ -233,19 +240,40 @@ __attribute__((visibility("default"))) int refp_ppr(void* h, uint32_t src, uint3
   }
   const auto lines = stop_capture();
   *epochs = epoch_deltas(lines, nullptr, 0);
-  *trace = 0;
-  if (pushpull) {
-    // the dual-mode PPR decides its own switch (personalized_pagerank.hpp:184-205):
-    // its epochs log no engine line; a push epoch is one whose engine call
-    // went through broadcast, counted from the "push" marker it leaves
-    uint64_t t = 0;
-    uint32_t e = 0;
-    for (const auto& l : lines) {
-      if (l.rfind("[epoch-", 0) == 0) ++e;
-      (void)t;
-    }
-    *trace = t;
+  return 0;
+}
+
+// algo::trustrank with select_good_seeds (trustrank.hpp:88-259): good [V]
+// 0/1 bytes; ranks [max_v_i + 1]; *epochs = the trust epochs (the last
+// "[epoch-i]" lines after the selection PageRank's).  select_method 2 draws
+// from std::random_device in the reference and is not offered here.
+__attribute__((visibility("default"))) int refp_trustrank(void* h, const uint8_t* good, uint32_t seed_num,
+                                                          uint32_t select_method, uint32_t iteration,
+                                                          double damping, double eps, double* out,
+                                                          uint32_t* epochs) {
+  auto* g = static_cast<ref_graph*>(h);
+  if (select_method > 1) return 1;
+  plato::bitmap_t<> good_vertices(g->info.max_v_i_ + 1);
+  for (uint32_t v = 0; v <= g->info.max_v_i_; ++v)
+    if (good[v]) good_vertices.set_bit(v);
+  plato::algo::trustrank_opts_t opts;
+  opts.iteration_ = iteration;
+  opts.damping_ = damping;
+  opts.seed_num_ = seed_num;
+  opts.select_method_ = select_method;
+  opts.eps_ = eps;
+  start_capture();
+  auto ranks = plato::algo::trustrank(*g->dcsc, *g->bcsr, g->info, good_vertices, opts);
+  const auto lines = stop_capture();
+  copy_out(ranks, g->info.max_v_i_ + 1, out);
+  // the trust loop's epochs follow the selection PageRank's (if any): count
+  // the "[epoch-" lines after the last epoch-0 line
+  uint32_t n = 0;
+  for (const auto& l : lines) {
+    if (l.rfind("[epoch-0]", 0) == 0) n = 0;
+    if (l.rfind("[epoch-", 0) == 0) ++n;
   }
+  *epochs = n;
   return 0;
 }
 

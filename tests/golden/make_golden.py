@@ -12,7 +12,14 @@ lines skipped) and writes
   hll_golden.npz  murmurhash3 values, HyperLogLog registers and estimates
                   computed by the reference's own plato/util/hash.hpp and
                   plato/util/hyperloglog.hpp (compiled from the reference tree
-                  by oracle/build.py build_ref into oracle/_ref/).
+                  by oracle/build.py build_ref into oracle/_ref/),
+  ref_golden.npz  the reference's own algo::pagerank, personalized_pagerank
+                  (pull-only and dual-mode), breadth_first_search and trustrank
+                  outputs on fixture graphs (the reference's engine path
+                  compiled into oracle/_ref/libplato_ref.so by build_ref; see
+                  oracle/refplato.py): ranks, epoch counts, per-epoch deltas,
+                  BFS visited counts, vertices activated per level and the
+                  engine's push/pull choice per level.
 The reference tree is only needed to regenerate; tests read the outputs.
 """
 from __future__ import annotations
@@ -131,6 +138,71 @@ def hll_vectors(root: Path) -> dict:
     return out
 
 
+REF_GRAPHS = {
+    # name: (fixture CSV or RMAT (scale, seed, symmetrise), is_directed)
+    "v100u": ("v100_e2150_ua_c3.csv", False),
+    "v100d": ("v100_e4300_da_c3.csv", True),
+    "rmat12d": ((12, 1, False), True),
+    "rmat12u": ((12, 2, True), False),
+    "rmat14d": ((14, 3, False), True),
+}
+
+
+def ref_graph_edges(root: Path, spec):
+    """Edge list of a REF_GRAPHS entry: a fixture CSV, or the oracle's seeded
+    RMAT generator (equal to the product's; edgefactor 16)."""
+    if isinstance(spec, str):
+        return parse_csv(root / "data" / "graph" / spec)
+    import oracle
+    scale, seed, sym = spec
+    _, s, d = oracle.rmat(scale, 16, seed, symmetrize=sym)
+    return s, d
+
+
+def ref_vectors(root: Path) -> dict:
+    """The reference's own outputs on REF_GRAPHS (oracle/_ref/libplato_ref.so)."""
+    sys.path.insert(0, str(HERE.parent.parent))
+    from oracle.build import build_ref
+    build_ref(ref_root=root)
+    from oracle.refplato import ReferenceGraph
+    out = {}
+    for name, (spec, directed) in REF_GRAPHS.items():
+        s, d = ref_graph_edges(root, spec)
+        V = int(max(s.max(), d.max())) + 1
+        g = ReferenceGraph(V, s, d, directed)
+        out[f"{name}__meta"] = np.array([g.vertices, g.max_v_i, g.edges, int(directed)], np.uint64)
+        r, ep, dl = g.pagerank(100, 0.85, 0.0)
+        out[f"{name}__pr100"], out[f"{name}__pr100_epochs"], out[f"{name}__pr100_deltas"] = r, ep, dl
+        r, ep, dl = g.pagerank(100, 0.85, 0.001)  # pagerank_opts_t defaults: early exit
+        out[f"{name}__preps"], out[f"{name}__preps_epochs"] = r, ep
+        deg = np.bincount(s, minlength=V) + (0 if directed else np.bincount(d, minlength=V))
+        src = int(np.random.default_rng(7).choice(np.flatnonzero(deg > 0)))
+        out[f"{name}__ppr_src"] = src
+        for mode, pp in (("pull", False), ("pp", True)):
+            r, ep = g.ppr(src, 200, 0.85, 1e-7, pp)
+            out[f"{name}__ppr_{mode}"], out[f"{name}__ppr_{mode}_epochs"] = r, ep
+        roots = np.random.default_rng(11).choice(np.flatnonzero(deg > 0), 3, replace=False)
+        vis, acts, trs = [], [], []
+        for rt in roots:
+            v, a, t = g.bfs(int(rt))
+            vis.append(v)
+            acts.append(np.pad(a, (0, 64 - a.size)))
+            trs.append(t)
+        out[f"{name}__bfs_roots"] = roots.astype(np.uint32)
+        out[f"{name}__bfs_visited"] = np.array(vis, np.uint64)
+        out[f"{name}__bfs_actives"] = np.stack(acts)
+        out[f"{name}__bfs_trace"] = np.array(trs, np.uint64)
+        good = (np.arange(V) % 5 == 0).astype(np.uint8)
+        out[f"{name}__good"] = good
+        r, ep = g.trustrank(good, V + 1, 0, 100, 0.85, 1e-6)  # every good vertex a seed
+        out[f"{name}__tr_all"], out[f"{name}__tr_all_epochs"] = r, ep
+        for m in (0, 1):
+            r, ep = g.trustrank(good, 20, m, 100, 0.85, 0.001)
+            out[f"{name}__tr_m{m}"], out[f"{name}__tr_m{m}_epochs"] = r, ep
+        g.close()
+    return {k: np.asarray(v) for k, v in out.items()}
+
+
 def main(root: Path) -> None:
     arrays = {}
     for name in GRAPHS:
@@ -147,7 +219,8 @@ def main(root: Path) -> None:
     np.savez_compressed(HERE / "fixtures.npz", **arrays)
     (HERE / "kats.json").write_text(json.dumps(KATS, indent=1) + "\n")
     np.savez_compressed(HERE / "hll_golden.npz", **hll_vectors(root))
-    print("wrote", HERE / "fixtures.npz", HERE / "kats.json", HERE / "hll_golden.npz")
+    np.savez_compressed(HERE / "ref_golden.npz", **ref_vectors(root))
+    print("wrote", HERE / "fixtures.npz", HERE / "kats.json", HERE / "hll_golden.npz", HERE / "ref_golden.npz")
 
 
 if __name__ == "__main__":

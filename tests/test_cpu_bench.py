@@ -17,7 +17,7 @@ bench.run_reference(args)
 maps = open('/proc/self/maps').read()
 print(json.dumps({{"product_module": 'plato_b200' in sys.modules,
                    "product_so": 'libplato_b200' in maps,
-                   "oracle_so": 'libref_cpu' in maps}}))
+                   "oracle_so": 'libref_cpu' in maps or 'libplato_ref' in maps}}))
 """
 
 
@@ -28,8 +28,11 @@ def test_reference_arm_loads_no_product_code():
     lines = [json.loads(x) for x in out.stdout.strip().splitlines()]
     line, probe = lines[0], lines[1]
     assert line["impl"] == "reference" and line["unit"] == "GTEPS" and line["value"] > 0
-    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "port"
-    assert probe == {"product_module": False, "product_so": False, "oracle_so": True}
+    from oracle import refplato
+    assert line["e2e"]["h2d_bytes_per_step"] == 0
+    assert line["cpu_baseline"]["kind"] == ("reference" if refplato.available() else "port")
+    assert not probe["product_module"] and not probe["product_so"]
+    assert probe["oracle_so"]
 
 
 def test_both_arms_share_one_config():
