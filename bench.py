@@ -834,6 +834,46 @@ def _serve(pb, g, sets, rates, n_req, slots):
     return out
 
 
+CEILING_MODES = ["ids", "gather4", "gather8", "gather16", "hot_l1", "coalesced"]
+
+
+def run_ceiling(args):
+    """The long-bin gather stream's ceiling on this GPU (plato_diag_pull_ceiling
+    modes 0-5) beside the real k_pull_long, on the benchmark graph: one JSON
+    line.  Times are CUDA-event averages per launch."""
+    import ctypes as C
+
+    import torch
+    import plato_b200 as pb
+    from plato_b200 import _lib
+    lib = _lib.load()
+    V, src, dst = pb.rmat(SCALE, EDGEFACTOR, SEED)
+    g = pb.Graph(V, src, dst, is_directed=True)
+    bins = pull_bins(V, dst)
+    del src, dst
+    out = {"ceiling": True, "workload": f"pagerank_rmat_s{SCALE}_ef{EDGEFACTOR}_seed{SEED}", "vertices": V,
+           "long_bin": {"rows": bins["rows"]["k_pull_long"], "edges": bins["edges"]["k_pull_long"],
+                        "algorithmic_bytes": bins["k_pull_long"]}}
+    peak, kind = measured_peak()
+    for mode, name in enumerate(CEILING_MODES):
+        ms, n, cs = C.c_double(), C.c_uint64(), C.c_double()
+        _lib.check(lib.plato_diag_pull_ceiling(g.handle, mode, 20, C.byref(ms), C.byref(n), C.byref(cs)),
+                   "plato_diag_pull_ceiling")
+        out[name] = {"ms": ms.value, "edges": n.value, "edges_per_ns": n.value / (ms.value * 1e6),
+                     "frac_if_long_bin": bins["k_pull_long"] / (ms.value / 1e3) / 1e9 / peak}
+    d_out = torch.empty(V, dtype=torch.float32, device="cuda")
+    g.pagerank_device(d_out.data_ptr(), ITERATIONS, DAMPING, 0.0)
+    kt = _profiled(pb, ["k_pull_long"], lambda: g.pagerank_device(d_out.data_ptr(), ITERATIONS, DAMPING, 0.0))
+    torch.cuda.synchronize()
+    tot, n = kt["k_pull_long"]
+    out["k_pull_long"] = {"ms": tot / n, "edges_per_ns": bins["edges"]["k_pull_long"] / (tot / n * 1e6),
+                          "frac": bins["k_pull_long"] / (tot / n / 1e3) / 1e9 / peak}
+    out["peak"] = {"hbm_gbs": peak, "source": kind}
+    g.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_suite(args):
     import torch  # noqa: F401  (CUDA context for the library)
     import plato_b200 as pb
@@ -866,10 +906,14 @@ def main():
                     help="also measure BFS, single PPR, batched PPR and serving (one JSON line each)")
     ap.add_argument("--only", default="", help="with --suite: comma list of bfs,cc,trustrank,hll,wpr,ppr_single,ppr_batch,serving")
     ap.add_argument("--quick", action="store_true", help="with --suite: one small batch (profiling)")
+    ap.add_argument("--ceiling", action="store_true",
+                    help="measure the long-bin gather stream's ceiling beside k_pull_long (one JSON line)")
     args = ap.parse_args()
     globals()["SCALE"] = args.scale
     if args.suite:
         return run_suite(args)
+    if args.ceiling:
+        return run_ceiling(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_plato(args)

@@ -303,6 +303,20 @@ int plato_pagerank_csc_noalloc(uint32_t vertices, uint64_t edges, const uint64_t
                                const plato_pagerank_opts* opts, float* d_ranks, void* stream,
                                plato_run_stats* stats);
 
+/* ---- diagnostics -----------------------------------------------------------
+ * No counterpart in the reference.  The memory system's rate on this graph's
+ * long-bin pull gather stream (the CSC source ids of rows with in-degree > 64,
+ * one 4-byte rank gathered per id), with the row bookkeeping and the update
+ * taken out: mode 0 the id stream alone; 1 / 2 / 3 ids + random gathers with
+ * 4 / 8 / 16 in flight per lane; 4 gathers folded into the first 64K ranks
+ * (L1-resident); 5 gathers at the edge position mod V (coalesced).
+ * *ms_per_launch = CUDA-event average over `reps` launches after 3 warm-ups;
+ * *edges = ids in the stream; *checksum keeps the loads live.  The graph must
+ * be relabelled (the default).  Allocates and synchronises: not for hot
+ * paths. */
+int plato_diag_pull_ceiling(plato_graph* g, uint32_t mode, uint32_t reps, double* ms_per_launch,
+                            uint64_t* edges, double* checksum);
+
 /* ---- batched multi-source personalized pagerank --------------------------
  * K queries, query q's seed set is seeds[seed_offsets[q] .. seed_offsets[q+1]).
  * Each query follows the seed-set semantics of algo::trustrank

@@ -127,6 +127,8 @@ SIGNATURES = {
     "plato_pagerank_device": (C.c_int, [P, C.POINTER(PagerankOpts), P, P, C.POINTER(RunStats)]),
     "plato_pagerank_csc_noalloc": (C.c_int, [C.c_uint32, C.c_uint64, P, P, P,
                                              C.POINTER(PagerankOpts), P, P, C.POINTER(RunStats)]),
+    "plato_diag_pull_ceiling": (C.c_int, [P, C.c_uint32, C.c_uint32, C.POINTER(C.c_double),
+                                          C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
     "plato_ppr_batch_k_tile": (C.c_int, [P, C.c_uint32, C.POINTER(C.c_uint32)]),
     "plato_ppr_batch": (C.c_int, [P, C.c_uint32, P, P, C.POINTER(PprBatchOpts), P, P, P, P]),
     "plato_server_create": (C.c_int, [P, C.POINTER(ServerOpts), C.POINTER(P)]),

@@ -1,0 +1,145 @@
+// Pull-gather ceiling: what the memory system gives this graph's gather
+// stream when nothing else is in the way.
+//
+// The long-bin pull kernel (k_pull_long) reads the CSC source ids of rows
+// with in-degree > 64 as a coalesced stream and gathers one 4-byte rank per
+// id at a random place in the rank vector.  These diagnostic kernels run the
+// same id stream (the first row past in-degree 64 bounds it) with the
+// row bookkeeping, the update and the delta taken out, so their times bound
+// what any kernel with this access pattern can reach on this GPU:
+//   0 ids      the id stream alone (16-byte coalesced loads): the DRAM part
+//   1 gather4  ids + gathers, 4 ranks in flight per lane (k_pull_long's depth)
+//   2 gather8  8 in flight per lane
+//   3 gather16 16 in flight per lane
+//   4 hot      as gather8 with every id folded into the first 64K ranks
+//              (256 KB, L1-resident; fewer on graphs below 64K vertices):
+//              the L1 rate for divergent gathers
+//   5 coalesced as gather8 with the gather at the edge's own position mod V:
+//              the same instruction mix with coalesced gathers
+// Each launch runs a fixed grid (8 CTAs x 256 threads per SM; the 16-deep
+// variant fits 4 CTAs at a time at its register count) over 32*M-edge
+// chunks; a checksum per CTA keeps the loads live.  No counterpart in the
+// reference; it serves the roofline analysis only.
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "graph.cuh"
+
+namespace plato_b200 {
+namespace {
+
+__global__ void __launch_bounds__(256, 8) k_ceil_ids(const uint32_t* __restrict__ adj, uint64_t n,
+                                                     uint32_t* __restrict__ sink) {
+  const uint64_t n4 = n / 4;
+  const uint4* a4 = reinterpret_cast<const uint4*>(adj);
+  uint32_t acc = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n4; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint4 v = __ldcs(a4 + i);
+    acc ^= v.x ^ v.y ^ v.z ^ v.w;
+  }
+  acc = __reduce_xor_sync(0xffffffffu, acc);
+  if ((threadIdx.x & 31) == 0) atomicXor(sink + blockIdx.x, acc);
+}
+
+// kMode: 0 random gathers, 1 ids folded into the first 64K ranks, 2 gather at
+// the edge position mod V.
+template <int M, int kMode>
+__global__ void __launch_bounds__(256, (M <= 8 ? 8 : 4)) k_ceil_gather(const uint32_t* __restrict__ adj, uint64_t n,
+                                                        const float* __restrict__ x, uint32_t V,
+                                                        uint32_t hot_mask, float* __restrict__ sink) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  const uint64_t chunk = 32ull * M;
+  float s = 0.f;
+  for (uint64_t c = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; c * chunk < n; c += nwarps) {
+    const uint64_t b = c * chunk + lane;
+    uint32_t id[M];
+#pragma unroll
+    for (int k = 0; k < M; ++k) {
+      const uint64_t e = b + 32ull * k;
+      uint32_t v = e < n ? __ldcs(adj + e) : 0u;
+      if (kMode == 1) v &= hot_mask;  // hot_mask + 1 <= V
+      if (kMode == 2) v = static_cast<uint32_t>(e % V);
+      id[k] = v;
+    }
+#pragma unroll
+    for (int k = 0; k < M; ++k) s += (b + 32ull * k < n) ? __ldg(x + id[k]) : 0.f;
+  }
+  s = warp_sum(s);
+  if (lane == 0) atomicAdd(sink + blockIdx.x, s);
+}
+
+}  // namespace
+}  // namespace plato_b200
+
+using namespace plato_b200;
+
+extern "C" int plato_diag_pull_ceiling(plato_graph* g, uint32_t mode, uint32_t reps, double* ms_per_launch,
+                                       uint64_t* edges, double* checksum) {
+  if (!g || !ms_per_launch || mode > 5 || reps == 0)
+    return set_error(PLATO_EINVAL, "plato_diag_pull_ceiling: bad argument");
+  if (!g->relabeled) return set_error(PLATO_EINVAL, "plato_diag_pull_ceiling: the graph must be relabelled");
+  std::lock_guard<std::mutex> lock(g->mu);
+  try {
+    PLATO_CUDA_TRY(cudaSetDevice(g->device));
+    const uint32_t V = g->info.vertices;
+    cudaStream_t st = g->stream;
+    // rows are numbered by descending in-degree: the long bin is [0, n_long)
+    std::vector<uint32_t> deg(V);
+    PLATO_CUDA_TRY(cudaMemcpy(deg.data(), g->in_deg.p, 4ull * V, cudaMemcpyDeviceToHost));
+    const uint32_t n_long = static_cast<uint32_t>(
+        std::upper_bound(deg.begin(), deg.end(), 64u, [](uint32_t a, uint32_t b) { return a > b; }) - deg.begin());
+    uint64_t n = 0;
+    PLATO_CUDA_TRY(cudaMemcpy(&n, g->in_off.p + n_long, 8, cudaMemcpyDeviceToHost));
+    if (edges) *edges = n;
+    int sms = 0;
+    PLATO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
+    const unsigned grid = 8u * static_cast<unsigned>(sms);
+    uint32_t hot_mask = 1u << 16;  // a power of two <= min(V, 64K), minus one
+    while (hot_mask > V) hot_mask >>= 1;
+    hot_mask -= 1;
+    dbuf<float> x;
+    dbuf<float> sink;
+    PLATO_TRY(x.alloc(V));
+    PLATO_TRY(sink.alloc(grid));
+    std::vector<float> h_x(V, 1.0f / V);
+    PLATO_CUDA_TRY(cudaMemcpy(x.p, h_x.data(), 4ull * V, cudaMemcpyHostToDevice));
+    PLATO_CUDA_TRY(cudaMemset(sink.p, 0, 4ull * grid));
+    auto launch = [&]() {
+      switch (mode) {
+        case 0: k_ceil_ids<<<grid, 256, 0, st>>>(g->in_adj.p, n, reinterpret_cast<uint32_t*>(sink.p)); break;
+        case 1: k_ceil_gather<4, 0><<<grid, 256, 0, st>>>(g->in_adj.p, n, x.p, V, hot_mask, sink.p); break;
+        case 2: k_ceil_gather<8, 0><<<grid, 256, 0, st>>>(g->in_adj.p, n, x.p, V, hot_mask, sink.p); break;
+        case 3: k_ceil_gather<16, 0><<<grid, 256, 0, st>>>(g->in_adj.p, n, x.p, V, hot_mask, sink.p); break;
+        case 4: k_ceil_gather<8, 1><<<grid, 256, 0, st>>>(g->in_adj.p, n, x.p, V, hot_mask, sink.p); break;
+        default: k_ceil_gather<8, 2><<<grid, 256, 0, st>>>(g->in_adj.p, n, x.p, V, hot_mask, sink.p); break;
+      }
+      count_launch();
+    };
+    for (int w = 0; w < 3; ++w) launch();
+    cudaEvent_t e0, e1;
+    PLATO_CUDA_TRY(cudaEventCreate(&e0));
+    PLATO_CUDA_TRY(cudaEventCreate(&e1));
+    PLATO_CUDA_TRY(cudaEventRecord(e0, st));
+    for (uint32_t r = 0; r < reps; ++r) launch();
+    PLATO_CUDA_TRY(cudaEventRecord(e1, st));
+    PLATO_CUDA_TRY(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    PLATO_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    PLATO_CUDA_TRY(cudaGetLastError());
+    *ms_per_launch = static_cast<double>(ms) / reps;
+    if (checksum) {
+      std::vector<float> h(grid);
+      PLATO_CUDA_TRY(cudaMemcpy(h.data(), sink.p, 4ull * grid, cudaMemcpyDeviceToHost));
+      double cs = 0.0;
+      for (float v : h) cs += v;
+      *checksum = cs;
+    }
+  } catch (const std::exception& ex) {
+    return set_error(PLATO_ECUDA, std::string("plato_diag_pull_ceiling: ") + ex.what());
+  }
+  return PLATO_OK;
+}
