@@ -88,8 +88,9 @@ extern "C" int plato_diag_pull_ceiling(plato_graph* g, uint32_t mode, uint32_t r
     // rows are numbered by descending in-degree: the long bin is [0, n_long)
     std::vector<uint32_t> deg(V);
     PLATO_CUDA_TRY(cudaMemcpy(deg.data(), g->in_deg.p, 4ull * V, cudaMemcpyDeviceToHost));
+    // first row with in-degree <= 64 (the array is non-increasing)
     const uint32_t n_long = static_cast<uint32_t>(
-        std::upper_bound(deg.begin(), deg.end(), 64u, [](uint32_t a, uint32_t b) { return a > b; }) - deg.begin());
+        std::partition_point(deg.begin(), deg.end(), [](uint32_t e) { return e > 64u; }) - deg.begin());
     uint64_t n = 0;
     PLATO_CUDA_TRY(cudaMemcpy(&n, g->in_off.p + n_long, 8, cudaMemcpyDeviceToHost));
     if (edges) *edges = n;
