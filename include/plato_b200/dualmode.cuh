@@ -36,6 +36,15 @@
  *   switch  active_edges = sum of out-degrees over `actives`; push iff
  *         active_edges / edges < push_threshold, edges doubled for undirected
  *         graphs (dualmode.hpp:261-279).
+ *   pull with a combiner (opt-in: the overloads that take
+ *         make_combiner(f), f(MSG& into, const MSG& from)): the in-adjacency
+ *         is split into pieces of at most kPiece (4) edges, consecutive
+ *         lanes of a warp take consecutive pieces (a warp reads up to 128
+ *         contiguous ids), each piece is one signal call, and the messages
+ *         of one vertex within a warp are folded with f in lane order before
+ *         one slot call per vertex and warp.  f must be associative; a
+ *         signal's messages must be for its own vertex v.  Without a
+ *         combiner the 64-edge path above runs.
  * Vertex ids seen by functors are the engine's internal ids; states copied to
  * the host with to_host() are returned in caller ids.
  */
@@ -46,6 +55,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include <cstdint>
+#include <cstring>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -59,6 +69,17 @@ using vid_t = uint32_t;
 using eid_t = uint64_t;
 
 constexpr uint32_t kPullChunk = 64;
+constexpr uint32_t kPiece = 4;  // edges per signal call on the combined pull
+
+// Message combiner of the combined pull: f(MSG& into, const MSG& from).
+template <typename F>
+struct combiner {
+  F f;
+};
+template <typename F>
+combiner<F> make_combiner(F f) {
+  return combiner<F>{f};
+}
 
 struct adj_unit_t {  // adj_unit_t<empty_t> (plato/graph/base.hpp)
   vid_t neighbour_;
@@ -338,6 +359,127 @@ __global__ void k_push(const vid_t* queue, uint64_t n, SIG sig, SLOT slot, R* re
   if (acc != R()) reduce_add(acc, result);
 }
 
+// Pieces of the combined pull.  Columns with in-edges are listed in vertex
+// order (colv) with the index of their first piece (pstart, a column of d
+// edges has ceil(d / kPiece) pieces); wstart[w] is the column holding piece
+// 32w, the first piece of warp w.
+static __global__ void k_piece_flags(const uint64_t* off, uint32_t V, uint32_t* flag) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+       v += (uint64_t)gridDim.x * blockDim.x)
+    flag[v] = off[v + 1] > off[v] ? 1u : 0u;
+}
+
+static __global__ void k_piece_cols(const uint64_t* off, uint32_t V, const uint32_t* cidx, vid_t* colv,
+                                    uint64_t* npieces) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t d = off[v + 1] - off[v];
+    if (d == 0) continue;
+    colv[cidx[v]] = static_cast<vid_t>(v);
+    npieces[cidx[v]] = (d + kPiece - 1) / kPiece;
+  }
+}
+
+static __global__ void k_piece_warps(const uint64_t* pstart, uint32_t ncols, uint32_t* wstart) {
+  for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < ncols;
+       c += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t ps = pstart[c], pe = pstart[c + 1];
+    for (uint64_t w = (ps + 31) / 32; w * 32 < pe; ++w) wstart[w] = static_cast<uint32_t>(c);
+  }
+}
+
+// Lane-to-lane shift of any trivially copyable message (whole 32-bit words).
+template <typename T>
+__device__ __forceinline__ T shfl_up_any(const T& v, unsigned d) {
+  static_assert(sizeof(T) % 4 == 0, "combined pull: message size must be a multiple of 4 bytes");
+  constexpr int kWords = sizeof(T) / 4;
+  uint32_t w[kWords];
+  memcpy(w, &v, sizeof(T));
+#pragma unroll
+  for (int i = 0; i < kWords; ++i) w[i] = __shfl_up_sync(0xffffffffu, w[i], d);
+  T out;
+  memcpy(&out, w, sizeof(T));
+  return out;
+}
+
+// Context of a combined pull signal: its messages fold into one per lane.
+template <typename MSG, typename COMB>
+struct combine_context {
+  const COMB* comb;
+  MSG* msg;
+  bool* has;
+  __device__ void send(const mepa_ag_message_t<MSG>& m) const {
+    if (*has) {
+      comb->f(*msg, m.message_);
+    } else {
+      *msg = m.message_;
+      *has = true;
+    }
+  }
+};
+
+template <typename MSG, typename R, typename SIG, typename SLOT, typename COMB>
+__global__ void __launch_bounds__(256) k_pull_combined(const vid_t* __restrict__ colv,
+                                                       const uint64_t* __restrict__ pstart,
+                                                       const uint32_t* __restrict__ wstart, uint32_t ncols,
+                                                       uint64_t npieces, const uint64_t* __restrict__ off,
+                                                       const vid_t* __restrict__ adj, SIG sig, SLOT slot,
+                                                       COMB comb, R* result) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  R acc = R();
+  for (uint64_t w = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; w * 32 < npieces; w += nwarps) {
+    const uint64_t p = w * 32 + lane;
+    const bool valid = p < npieces;
+    // column of each lane: c0 holds piece 32w; a later column starting at
+    // relative piece r sets bit r, and lane l lies in column c0 + (bits <= l)
+    const uint32_t c0 = wstart[w];
+    const uint32_t cb = c0 + 1 + lane;
+    const uint64_t b = cb <= ncols ? pstart[cb] : ~0ull;
+    const uint64_t r = b - w * 32;
+    const uint32_t bits = __reduce_or_sync(0xffffffffu, r < 32 ? (1u << r) : 0u);
+    const uint32_t upto = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
+    const uint32_t col = c0 + static_cast<uint32_t>(__popc(bits & upto));
+    MSG msg{};
+    bool has = false;
+    vid_t v = 0;
+    if (valid) {
+      v = colv[col];
+      const uint64_t e0 = off[v] + (p - pstart[col]) * kPiece;
+      const uint64_t e1 = min(e0 + kPiece, off[v + 1]);
+      const adj_unit_list_t adjs{reinterpret_cast<const adj_unit_t*>(adj + e0),
+                                 reinterpret_cast<const adj_unit_t*>(adj + e1)};
+      combine_context<MSG, COMB> ctx{&comb, &msg, &has};
+      sig(ctx, v, adjs);
+    }
+    // segmented inclusive scan over lanes of the same column, in lane order
+    const uint32_t key = valid ? col : 0xffffffffu;
+#pragma unroll
+    for (unsigned d = 1; d < 32; d <<= 1) {
+      const MSG om = shfl_up_any(msg, d);
+      const uint32_t ok = __shfl_up_sync(0xffffffffu, key, d);
+      const bool oh = __shfl_up_sync(0xffffffffu, has ? 1u : 0u, d) != 0u;
+      if (lane >= d && ok == key && oh) {
+        if (has) {
+          MSG t = om;
+          comb.f(t, msg);
+          msg = t;
+        } else {
+          msg = om;
+          has = true;
+        }
+      }
+    }
+    const uint32_t nk = __shfl_down_sync(0xffffffffu, key, 1);
+    const bool tail = lane == 31 || nk != key;
+    if (valid && has && tail) {
+      mepa_ag_message_t<MSG> m{v, msg};
+      acc += slot(0, m);
+    }
+  }
+  if (acc != R()) reduce_add(acc, result);
+}
+
 }  // namespace detail
 
 template <typename T>
@@ -367,6 +509,11 @@ class dualmode_engine_t {
   dualmode_engine_t(const dualmode_engine_t&) = delete;
   dualmode_engine_t& operator=(const dualmode_engine_t&) = delete;
   ~dualmode_engine_t() {
+    for (auto& pi : pieces_) {
+      dev_free(pi.colv);
+      dev_free(pi.pstart);
+      dev_free(pi.wstart);
+    }
     dev_free(chunks_);
     dev_free(queue_);
     dev_free(counters_);
@@ -430,6 +577,20 @@ class dualmode_engine_t {
     check_cuda(cudaGetLastError(), "pull launch");
   }
 
+  // pull only with a message combiner (see the header comment)
+  template <typename MSG, typename R, typename PULL_SIGNAL, typename PULL_SLOT, typename F>
+  R foreach_edges(PULL_SIGNAL signal, PULL_SLOT slot, combiner<F> comb) {
+    R* res = result_buf<R>();
+    pull_combined<MSG, R>(signal, slot, comb, res);
+    return read_result<R>(res);
+  }
+
+  // as foreach_edges_device above, with a message combiner
+  template <typename MSG, typename R, typename PULL_SIGNAL, typename PULL_SLOT, typename F>
+  void foreach_edges_device(PULL_SIGNAL signal, PULL_SLOT slot, combiner<F> comb, R* d_result) {
+    pull_combined<MSG, R>(signal, slot, comb, d_result);
+  }
+
   // push only (dualmode.hpp:311-322)
   template <typename MSG, typename R, typename PUSH_SIGNAL, typename PUSH_SLOT>
   R foreach_edges(PUSH_SIGNAL signal, PUSH_SLOT slot, bitmap_t& actives) {
@@ -450,6 +611,20 @@ class dualmode_engine_t {
     last_push_ = (static_cast<double>(active_edges) / static_cast<double>(edges)) < opts_.push_threshold_;
     if (last_push_) return push_queue<MSG, R>(push_signal, push_slot, n);
     return foreach_edges<MSG, R>(pull_signal, pull_slot);
+  }
+
+  // push + pull, engine-chosen, the pull with a message combiner
+  template <typename MSG, typename R, typename PUSH_SIGNAL, typename PUSH_SLOT,
+            typename PULL_SIGNAL, typename PULL_SLOT, typename F>
+  R foreach_edges(PUSH_SIGNAL push_signal, PUSH_SLOT push_slot, PULL_SIGNAL pull_signal,
+                  PULL_SLOT pull_slot, bitmap_t& actives, combiner<F> comb) {
+    uint64_t n = 0, active_edges = 0;
+    compact(actives, &n, &active_edges);
+    uint64_t edges = info_.edges;
+    if (!info_.is_directed) edges *= 2;
+    last_push_ = (static_cast<double>(active_edges) / static_cast<double>(edges)) < opts_.push_threshold_;
+    if (last_push_) return push_queue<MSG, R>(push_signal, push_slot, n);
+    return foreach_edges<MSG, R>(pull_signal, pull_slot, comb);
   }
 
   bool last_was_push() const { return last_push_; }
@@ -496,6 +671,65 @@ class dualmode_engine_t {
     chunks_reversed_ = reversed_;
   }
 
+  // The piece index of the pull direction (combined pull), built on the
+  // device: non-empty columns compacted with a scan, their piece counts
+  // scanned into first-piece offsets, then the first column of every warp.
+  void ensure_pieces() {
+    piece_index& pi = pieces_[reversed_ ? 1 : 0];
+    if (pi.built) return;
+    const uint32_t V = view_.vertices;
+    uint32_t* flag = nullptr;
+    uint32_t* cidx = nullptr;
+    uint64_t* cnt = nullptr;
+    void* tmp = nullptr;
+    size_t tmp_bytes = 0, t2 = 0;
+    dev_alloc(&flag, 4ull * (V ? V : 1), "pieces");
+    dev_alloc(&cidx, 4ull * (V + 1), "pieces");
+    detail::k_piece_flags<<<grid(V), 256>>>(in_off(), V, flag);
+    check_cuda(cudaMemset(cidx, 0, 4), "pieces");
+    check_cuda(cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, flag, cidx + 1, static_cast<int64_t>(V)), "pieces");
+    dev_alloc(&tmp, tmp_bytes, "pieces");
+    check_cuda(cub::DeviceScan::InclusiveSum(tmp, tmp_bytes, flag, cidx + 1, static_cast<int64_t>(V)), "pieces");
+    uint32_t ncols = 0;
+    check_cuda(cudaMemcpy(&ncols, cidx + V, 4, cudaMemcpyDeviceToHost), "pieces");
+    pi.ncols = ncols;
+    dev_alloc(&pi.colv, 4ull * (ncols ? ncols : 1), "pieces");
+    dev_alloc(&cnt, 8ull * (ncols ? ncols : 1), "pieces");
+    dev_alloc(&pi.pstart, 8ull * (ncols + 1), "pieces");
+    detail::k_piece_cols<<<grid(V), 256>>>(in_off(), V, cidx, pi.colv, cnt);
+    check_cuda(cudaMemset(pi.pstart, 0, 8), "pieces");
+    check_cuda(cub::DeviceScan::InclusiveSum(nullptr, t2, cnt, pi.pstart + 1, static_cast<int64_t>(ncols)), "pieces");
+    if (t2 > tmp_bytes) {
+      dev_free(tmp);
+      dev_alloc(&tmp, t2, "pieces");
+    }
+    if (ncols)
+      check_cuda(cub::DeviceScan::InclusiveSum(tmp, t2, cnt, pi.pstart + 1, static_cast<int64_t>(ncols)), "pieces");
+    uint64_t np = 0;
+    check_cuda(cudaMemcpy(&np, pi.pstart + ncols, 8, cudaMemcpyDeviceToHost), "pieces");
+    pi.npieces = np;
+    const uint64_t nw = (np + 31) / 32;
+    dev_alloc(&pi.wstart, 4ull * (nw ? nw : 1), "pieces");
+    if (ncols) detail::k_piece_warps<<<grid(ncols), 256>>>(pi.pstart, ncols, pi.wstart);
+    check_cuda(cudaGetLastError(), "pieces");
+    dev_free(tmp);
+    dev_free(flag);
+    dev_free(cidx);
+    dev_free(cnt);
+    pi.built = true;
+  }
+
+  template <typename MSG, typename R, typename SIG, typename SLOT, typename F>
+  void pull_combined(SIG signal, SLOT slot, combiner<F> comb, R* res) {
+    ensure_pieces();
+    const piece_index& pi = pieces_[reversed_ ? 1 : 0];
+    if (pi.npieces == 0) return;
+    const uint64_t threads = (pi.npieces + 31) / 32 * 32;
+    detail::k_pull_combined<MSG, R><<<grid(threads), 256>>>(pi.colv, pi.pstart, pi.wstart, pi.ncols, pi.npieces,
+                                                             in_off(), in_adj(), signal, slot, comb, res);
+    check_cuda(cudaGetLastError(), "combined pull launch");
+  }
+
   void compact(bitmap_t& actives, uint64_t* n, uint64_t* active_edges) {
     const uint32_t V = view_.vertices;
     if (!queue_) dev_alloc(&queue_, 4ull * (V ? V : 1), "queue");
@@ -532,6 +766,15 @@ class dualmode_engine_t {
     return h;
   }
 
+  struct piece_index {
+    bool built = false;
+    uint32_t ncols = 0;
+    uint64_t npieces = 0;
+    vid_t* colv = nullptr;
+    uint64_t* pstart = nullptr;
+    uint32_t* wstart = nullptr;
+  };
+
   plato_graph* g_;
   dualmode_engine_opts_t opts_;
   plato_graph_device_view view_{};
@@ -542,6 +785,7 @@ class dualmode_engine_t {
   vid_t* queue_ = nullptr;
   unsigned long long* counters_ = nullptr;
   void* result_ = nullptr;
+  piece_index pieces_[2];  // by direction: in-edges, out-edges (reversed)
 };
 
 }  // namespace plato_b200

@@ -9,7 +9,10 @@
 //               from v's own id) and sends it when below v's id; the slot
 //               lowers label[v] with write_min and activates v
 //       and the engine's active-edge switch picks push or pull; the loop ends
-//       after an epoch that lowered nothing.
+//       after an epoch that lowered nothing.  The pull runs on the engine's
+//       combined path: a vertex's 4-edge pieces in one warp fold to their
+//       smallest label before one slot call (the reference's slot sees one
+//       message per partition piece instead; write_min gives the same labels).
 //   summary (:247-340)  component count (distinct labels), the largest
 //       component ("major label"; ties here go to the smallest label, the
 //       reference takes whichever its hash map visits first) with its vertex
@@ -142,7 +145,11 @@ int cc_impl(plato_graph* g, const plato_dualmode_opts* eo, plato_vid_t* labels_o
           }
           return 0;
         },
-        active_current);
+        active_current,
+        // a vertex's pull messages fold to the smallest label before its slot
+        make_combiner([] __device__(cc_msg& into, const cc_msg& from) {
+          if (from.label_ < into.label_) into = from;
+        }));
     count_launch(2);
     if (engine.last_was_push()) {
       ++pushes;

@@ -20,6 +20,8 @@
 // precision, written with the reference's functor bodies for
 // include/plato_b200/dualmode.cuh (engine.reverse() for the transposed
 // graph), so the order of the ranks is the reference's up to FP64 rounding.
+// Its pulls run on the engine's combined path: the sums of a vertex's
+// 4-edge pieces in one warp are added in lane order before one write_add.
 #include <algorithm>
 #include <exception>
 #include <mutex>
@@ -198,7 +200,7 @@ std::vector<uint32_t> selection_top(plato_graph* g, bool inverse, uint32_t k) {
             atomicAdd(n + msg.v_i_, msg.message_);  // write_add (atomic.hpp:97-104)
             return 0;
           },
-          unused);
+          make_combiner([] __device__(double& into, const double& from) { into += from; }), unused);
       const int last = epoch + 1 == kIterations ? 1 : 0;
       k_tr_update<<<upd_blocks, 256>>>(n, c, deg, V, kDamping, last, delta, ctrl);
       check_cuda(cudaGetLastError(), "k_tr_update");

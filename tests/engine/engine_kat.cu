@@ -3,8 +3,11 @@
 // Test infrastructure: built into tests/engine/libengine_kat.so and driven by
 // tests/test_gpu_engine.py.  Each entry point restates one reference client
 // of dualmode_engine_t::foreach_edges with the same functor bodies:
-//   kat_aggregate   plato/graph/test/message_passing.cc:62-87 (AggregateMessage)
-//   kat_pagerank    plato/algo/pagerank/pagerank.hpp:81-146 (double state, write_add)
+//   kat_aggregate   plato/graph/test/message_passing.cc:62-87 (AggregateMessage),
+//                   also on the combined pull (messages of a vertex summed)
+//   kat_pagerank    plato/algo/pagerank/pagerank.hpp:81-146 (double state, write_add),
+//                   on the 64-edge or the combined pull, on the graph or its
+//                   transpose (engine.reverse())
 //   kat_bfs         plato/algo/bfs/bfs.hpp:70-151 (CAS parents, push/pull switch)
 #include <cstdio>
 #include <exception>
@@ -23,21 +26,23 @@ int fail(const std::exception& e) {
 
 extern "C" const char* kat_error() { return g_err.c_str(); }
 
-extern "C" int kat_aggregate(plato_graph* g, int32_t* values_out, int64_t* sum_out) {
+extern "C" int kat_aggregate(plato_graph* g, int combined, int32_t* values_out, int64_t* sum_out) {
   try {
     dualmode_engine_t engine(g);
     auto values = engine.alloc_v_state<int32_t>();
     values.fill(0);
     int32_t* vals = values.data();
-    const int32_t sum = engine.foreach_edges<uint32_t, int32_t>(
-        [] __device__(const auto& context, vid_t v_i, const adj_unit_list_t& adjs) {
-          for (auto it = adjs.begin_; adjs.end_ != it; ++it)
-            context.send(mepa_ag_message_t<uint32_t>{v_i, 1});
-        },
-        [vals] __device__(int, mepa_ag_message_t<uint32_t>& msg) -> int32_t {
-          atomicAdd(vals + msg.v_i_, static_cast<int32_t>(msg.message_));
-          return 1;
-        });
+    auto signal = [] __device__(const auto& context, vid_t v_i, const adj_unit_list_t& adjs) {
+      for (auto it = adjs.begin_; adjs.end_ != it; ++it) context.send(mepa_ag_message_t<uint32_t>{v_i, 1});
+    };
+    auto slot = [vals] __device__(int, mepa_ag_message_t<uint32_t>& msg) -> int32_t {
+      atomicAdd(vals + msg.v_i_, static_cast<int32_t>(msg.message_));
+      return static_cast<int32_t>(msg.message_);  // the messages this call stands for
+    };
+    const int32_t sum =
+        combined ? engine.foreach_edges<uint32_t, int32_t>(
+                       signal, slot, make_combiner([] __device__(uint32_t& a, const uint32_t& b) { a += b; }))
+                 : engine.foreach_edges<uint32_t, int32_t>(signal, slot);
     auto h = engine.to_host(values);
     for (size_t i = 0; i < h.size(); ++i) values_out[i] = h[i];
     *sum_out = sum;
@@ -47,13 +52,18 @@ extern "C" int kat_aggregate(plato_graph* g, int32_t* values_out, int64_t* sum_o
   }
 }
 
-extern "C" int kat_pagerank(plato_graph* g, uint32_t iterations, double damping, double* out) {
+extern "C" int kat_pagerank(plato_graph* g, uint32_t iterations, double damping, int combined, int reversed,
+                            double* out) {
   try {
     dualmode_engine_t engine(g);
+    if (reversed) engine.reverse();
     auto curt = engine.alloc_v_state<double>();
     auto next = engine.alloc_v_state<double>();
     const uint32_t V = engine.vertices();
-    const uint32_t* odeg = engine.out_degrees();
+    // out-degrees of the direction the pull walks (in-degrees on the transpose)
+    plato_graph_device_view view{};
+    plato_graph_get_device_view(g, &view);
+    const uint32_t* odeg = reversed ? view.in_degree : engine.out_degrees();
     // x = 1 / deg (pagerank.hpp:90-98): done with a push-only sweep over all vertices
     auto all = engine.alloc_v_subset();
     {
@@ -69,16 +79,20 @@ extern "C" int kat_pagerank(plato_graph* g, uint32_t iterations, double damping,
         [] __device__(int, int&) -> int { return 0; }, all);
     for (uint32_t epoch = 0; epoch < iterations; ++epoch) {
       next.fill(0.0);
-      engine.foreach_edges<double, int>(
-          [c] __device__(const auto& context, vid_t v_i, const adj_unit_list_t& adjs) {
-            double rank_sum = 0.0;
-            for (auto it = adjs.begin_; adjs.end_ != it; ++it) rank_sum += c[it->neighbour_];
-            context.send(mepa_ag_message_t<double>{v_i, rank_sum});
-          },
-          [n] __device__(int, mepa_ag_message_t<double>& msg) -> int {
-            atomicAdd(n + msg.v_i_, msg.message_);  // write_add (atomic.hpp:97-104)
-            return 0;
-          });
+      auto signal = [c] __device__(const auto& context, vid_t v_i, const adj_unit_list_t& adjs) {
+        double rank_sum = 0.0;
+        for (auto it = adjs.begin_; adjs.end_ != it; ++it) rank_sum += c[it->neighbour_];
+        context.send(mepa_ag_message_t<double>{v_i, rank_sum});
+      };
+      auto slot = [n] __device__(int, mepa_ag_message_t<double>& msg) -> int {
+        atomicAdd(n + msg.v_i_, msg.message_);  // write_add (atomic.hpp:97-104)
+        return 0;
+      };
+      if (combined)
+        engine.foreach_edges<double, int>(signal, slot,
+                                          make_combiner([] __device__(double& a, const double& b) { a += b; }));
+      else
+        engine.foreach_edges<double, int>(signal, slot);
       const bool last = epoch + 1 == iterations;
       engine.foreach_edges<int, int>(
           [n, odeg, d, last] __device__(const auto&, vid_t v) {

@@ -17,8 +17,8 @@ def kat():
     lib = C.CDLL(str(build()))
     P = C.c_void_p
     lib.kat_error.restype = C.c_char_p
-    lib.kat_aggregate.argtypes = [P, P, P]
-    lib.kat_pagerank.argtypes = [P, C.c_uint32, C.c_double, P]
+    lib.kat_aggregate.argtypes = [P, C.c_int, P, P]
+    lib.kat_pagerank.argtypes = [P, C.c_uint32, C.c_double, C.c_int, C.c_int, P]
     lib.kat_bfs.argtypes = [P, C.c_uint32, P, P, P]
     return lib
 
@@ -28,27 +28,45 @@ def _p(a):
 
 
 @pytest.mark.parametrize("relabel", [True, False])
-def test_aggregate_message_kat(kat, golden, relabel):
+@pytest.mark.parametrize("combined", [0, 1])
+def test_aggregate_message_kat(kat, golden, relabel, combined):
     graphs, kats = golden
     k = kats["aggregate_message"][0]
     g = graphs[k["graph"]]
     with pb.Graph(10, g["src"], g["dst"], True, relabel=relabel) as gr:
         vals = np.zeros(10, np.int32)
         total = C.c_int64()
-        assert kat.kat_aggregate(gr.handle, _p(vals), C.byref(total)) == 0, kat.kat_error()
+        assert kat.kat_aggregate(gr.handle, combined, _p(vals), C.byref(total)) == 0, kat.kat_error()
     assert total.value == k["sum"], k["source"]
     assert vals.tolist() == k["values"], k["source"]
 
 
 @pytest.mark.parametrize("directed", [True, False])
-def test_reference_pagerank_functors(kat, directed):
+@pytest.mark.parametrize("combined", [0, 1])
+@pytest.mark.parametrize("reversed_", [0, 1])
+def test_reference_pagerank_functors(kat, directed, combined, reversed_):
     V, s, d = pb.rmat(12, 16, 11, symmetrize=not directed)
-    ref = RefGraph(V, s, d, directed)
+    # the transpose's PageRank is the PageRank of the reversed edge list
+    ref = RefGraph(V, d, s, directed) if reversed_ else RefGraph(V, s, d, directed)
     want, _, _ = ref.pagerank(15, 0.85, 0.0)
     out = np.empty(V, np.float64)
     with pb.Graph(V, s, d, directed) as g:
-        assert kat.kat_pagerank(g.handle, 15, 0.85, _p(out)) == 0, kat.kat_error()
+        assert kat.kat_pagerank(g.handle, 15, 0.85, combined, reversed_, _p(out)) == 0, kat.kat_error()
     assert np.abs(out - want).max() <= 1e-9 * np.abs(want).max()
+
+
+def test_combined_pull_at_scale_matches_the_64_edge_pull(kat):
+    """The combined pull on a graph with hub columns spread over many warps
+    and long runs of short columns: PageRank equal to the 64-edge path's to
+    FP64 round-off, in both directions."""
+    V, s, d = pb.rmat(16, 16, 13)
+    with pb.Graph(V, s, d, True) as g:
+        for rev in (0, 1):
+            a = np.empty(V, np.float64)
+            b = np.empty(V, np.float64)
+            assert kat.kat_pagerank(g.handle, 10, 0.85, 0, rev, _p(a)) == 0, kat.kat_error()
+            assert kat.kat_pagerank(g.handle, 10, 0.85, 1, rev, _p(b)) == 0, kat.kat_error()
+            assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max()
 
 
 @pytest.mark.parametrize("directed", [True, False])
