@@ -303,6 +303,48 @@ int plato_pagerank_csc_noalloc(uint32_t vertices, uint64_t edges, const uint64_t
                                const plato_pagerank_opts* opts, float* d_ranks, void* stream,
                                plato_run_stats* stats);
 
+/* ---- 1D-partitioned PageRank over several GPUs ---------------------------
+ * The reference's multi-partition pull (create_dcsc_seqs_from_path with
+ * sequence_balanced_by_destination_t, plato/graph/structure.hpp:471-555,
+ * plato/graph/partition/sequence.hpp:43-75; one process per partition).
+ * Partition `rank` of `world` owns a set of destination vertices with all of
+ * their in-edges; the rank state the pull gathers is replicated on every GPU
+ * as a world x rows float array (internal global ids), each partition writes
+ * its slice [rank*rows, (rank+1)*rows) of the next state, and the caller
+ * assembles the next state with an all-gather (in place, equal counts: e.g.
+ * NCCL over NVLink) before the next epoch.  Vertices are ranked by descending
+ * in-degree (ties by caller id) and rank i goes to partition i % world at row
+ * i / world, so partitions hold equal row counts (some end in padding rows)
+ * and near-equal edge counts, and run the single-GPU degree-binned kernels.
+ * Every process passes the whole edge list (host memory) and derives the
+ * same layout.  PageRank semantics and units are plato_pagerank's. */
+typedef struct plato_partition plato_partition;
+/* Global internal id of every caller vertex (host [V]) and rows per partition,
+ * host-only (no GPU needed). */
+int plato_partition_layout(const plato_graph_info* info, const plato_vid_t* src, const plato_vid_t* dst,
+                           uint32_t world, plato_vid_t* global_ids, uint32_t* rows_per_partition);
+/* Builds partition `rank` on the current device. */
+int plato_partition_create(const plato_graph_info* info, const plato_vid_t* src, const plato_vid_t* dst,
+                           uint32_t rank, uint32_t world, plato_partition** out);
+int plato_partition_destroy(plato_partition* p);
+/* vertices = V of the whole graph, rows = rows per partition, real_rows = this
+ * partition's vertices (rows minus padding), edges = its in-edges. */
+int plato_partition_info(const plato_partition* p, uint32_t* vertices, uint32_t* rows, uint32_t* real_rows,
+                         uint64_t* edges);
+/* Writes this partition's slice of the initial state (pagerank.hpp:90-98,
+ * normalised) into d_state [world*rows] on `stream`. */
+int plato_partition_pagerank_init(plato_partition* p, float* d_state, double damping, void* stream);
+/* One pull epoch: gathers d_state [world*rows] (the assembled state), writes
+ * this partition's slice of d_next; final_epoch != 0 stores the ranks
+ * (pagerank.hpp:118-124).  d_delta (device, 1 double, or NULL) receives this
+ * partition's delta in normalised units (the reference's = sum over
+ * partitions x V); the caller sums it over partitions for the eps exit. */
+int plato_partition_pagerank_epoch(plato_partition* p, const float* d_state, float* d_next, double damping,
+                                   int final_epoch, double* d_delta, void* stream);
+/* Caller-id ranks (host [V]) from an assembled state copied to the host
+ * (h_state [world*rows]). */
+int plato_partition_ranks(const plato_partition* p, const float* h_state, float* ranks);
+
 /* ---- diagnostics -----------------------------------------------------------
  * No counterpart in the reference.  The memory system's rate on this graph's
  * long-bin pull gather stream (the CSC source ids of rows with in-degree > 64,

@@ -127,6 +127,15 @@ SIGNATURES = {
     "plato_pagerank_device": (C.c_int, [P, C.POINTER(PagerankOpts), P, P, C.POINTER(RunStats)]),
     "plato_pagerank_csc_noalloc": (C.c_int, [C.c_uint32, C.c_uint64, P, P, P,
                                              C.POINTER(PagerankOpts), P, P, C.POINTER(RunStats)]),
+    "plato_partition_layout": (C.c_int, [C.POINTER(GraphInfo), P, P, C.c_uint32, P, C.POINTER(C.c_uint32)]),
+    "plato_partition_create": (C.c_int, [C.POINTER(GraphInfo), P, P, C.c_uint32, C.c_uint32,
+                                         C.POINTER(C.c_void_p)]),
+    "plato_partition_destroy": (C.c_int, [P]),
+    "plato_partition_info": (C.c_int, [P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                       C.POINTER(C.c_uint64)]),
+    "plato_partition_pagerank_init": (C.c_int, [P, P, C.c_double, P]),
+    "plato_partition_pagerank_epoch": (C.c_int, [P, P, P, C.c_double, C.c_int, P, P]),
+    "plato_partition_ranks": (C.c_int, [P, P, P]),
     "plato_diag_pull_ceiling": (C.c_int, [P, C.c_uint32, C.c_uint32, C.POINTER(C.c_double),
                                           C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
     "plato_ppr_batch_k_tile": (C.c_int, [P, C.c_uint32, C.POINTER(C.c_uint32)]),

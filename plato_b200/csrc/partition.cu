@@ -1,0 +1,250 @@
+// 1D partitioned PageRank: the graph split by destination over several GPUs.
+//
+// Follows the reference's multi-partition layout for the pull engine
+// (create_dcsc_seqs_from_path, plato/graph/structure.hpp:471-555, with
+// sequence_balanced_by_destination_t, plato/graph/partition/sequence.hpp:43-75):
+// every partition owns a set of destination vertices with all of their
+// in-edges, and the rank state the pull gathers is replicated, refreshed
+// after every epoch by one exchange (the reference sends each pull message to
+// the owner through MPI, message_passing.hpp:88-144; here each partition
+// writes its own slice of the state and an all-gather over NCCL assembles the
+// next state on every GPU).
+//
+// Layout, B200 first: vertices are ranked by descending in-degree (ties by
+// caller id), the engine's own order, and position i goes to partition
+// i % P at local row i / P.  Every partition then holds the same number of
+// rows (n = ceil(V / P), the last rows of some partitions are padding), its
+// rows are still sorted by in-degree (so each runs the degree-binned pull
+// kernels unchanged), the edges are spread evenly (every partition takes one
+// of each P consecutive degree ranks), and the replicated state is one
+// P x n array in which partition r's rows sit at [r n, (r + 1) n): the
+// all-gather is in place with equal counts.  Global internal id of a vertex
+// = r n + local row; the CSC of a partition keeps its sources as global ids.
+//
+// Padding rows have no edges; their state is held at the value an edgeless
+// vertex keeps, (1 - d) / V, so they add nothing to any delta and nothing
+// gathers them.
+#include <omp.h>
+#include <parallel/algorithm>
+
+#include <algorithm>
+#include <new>
+#include <vector>
+
+#include "graph.cuh"
+#include "pull_merge.cuh"
+
+struct plato_partition {
+  plato_graph* g = nullptr;  // this partition's rows (internal; never handed out)
+  uint32_t rank = 0, world = 0, n = 0, real = 0, V = 0;
+  std::vector<uint32_t> gid;  // caller id -> global internal id
+  ~plato_partition() { delete g; }
+};
+
+namespace plato_b200 {
+
+// defined in rank.cu
+int partition_prepare(plato_graph* g, cudaStream_t st);
+int pull_epoch_partition(plato_graph* g, const float* x_gather, const float* x_old, float* xn, float tele,
+                         float d, bool final_epoch, cudaStream_t st, double* d_partial_sum);
+
+namespace {
+
+struct layout {
+  uint32_t V = 0, world = 0, n = 0;
+  std::vector<uint32_t> gid;  // caller id -> global internal id
+  std::vector<uint32_t> indeg, outdeg;  // by caller id (undirected: both = degree)
+};
+
+int make_layout(const plato_graph_info* info, const uint32_t* src, const uint32_t* dst, uint32_t world,
+                layout* L) {
+  const uint32_t V = info->vertices;
+  const uint64_t m = info->edges;
+  L->V = V;
+  L->world = world;
+  L->n = static_cast<uint32_t>((static_cast<uint64_t>(V) + world - 1) / world);
+  L->indeg.assign(V, 0);
+  L->outdeg.assign(V, 0);
+  for (uint64_t i = 0; i < m; ++i) {
+    if (src[i] >= V || dst[i] >= V) return set_error(PLATO_EINVAL, "partition: vertex id >= vertices");
+    ++L->indeg[dst[i]];
+    ++L->outdeg[src[i]];
+    if (!info->is_directed) {
+      ++L->indeg[src[i]];
+      ++L->outdeg[dst[i]];
+    }
+  }
+  std::vector<uint32_t> order(V);
+  for (uint32_t v = 0; v < V; ++v) order[v] = v;
+  const std::vector<uint32_t>& deg = L->indeg;
+  __gnu_parallel::sort(order.begin(), order.end(),
+                       [&deg](uint32_t a, uint32_t b) { return deg[a] != deg[b] ? deg[a] > deg[b] : a < b; });
+  L->gid.assign(V, 0);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < static_cast<int64_t>(V); ++i)
+    L->gid[order[i]] = static_cast<uint32_t>((i % world) * L->n + i / world);
+  return PLATO_OK;
+}
+
+__global__ void k_part_init(const uint32_t* __restrict__ deg, uint32_t rows, uint32_t real, uint32_t V,
+                            float ghost, float* x) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < rows;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t dg = deg[v];
+    x[v] = v >= real ? ghost : static_cast<float>(dg > 0 ? 1.0 / (static_cast<double>(V) * dg) : 1.0 / V);
+  }
+}
+
+}  // namespace
+}  // namespace plato_b200
+
+
+using namespace plato_b200;
+
+extern "C" int plato_partition_layout(const plato_graph_info* info, const plato_vid_t* src,
+                                      const plato_vid_t* dst, uint32_t world, plato_vid_t* global_ids,
+                                      uint32_t* rows_per_partition) {
+  if (!info || !global_ids || !rows_per_partition || (info->edges > 0 && (!src || !dst)))
+    return set_error(PLATO_EINVAL, "plato_partition_layout: null argument");
+  if (info->vertices == 0 || world == 0) return set_error(PLATO_EINVAL, "plato_partition_layout: empty");
+  try {
+    layout L;
+    PLATO_TRY(make_layout(info, src, dst, world, &L));
+    std::copy(L.gid.begin(), L.gid.end(), global_ids);
+    *rows_per_partition = L.n;
+  } catch (const std::bad_alloc&) {
+    return set_error(PLATO_ENOMEM, "plato_partition_layout: host allocation failed");
+  }
+  return PLATO_OK;
+}
+
+namespace plato_b200 {
+namespace {
+
+int build_partition(const plato_graph_info* info, const plato_vid_t* src, const plato_vid_t* dst, uint32_t rank,
+                    uint32_t world, plato_partition* p) {
+  layout L;
+  PLATO_TRY(make_layout(info, src, dst, world, &L));
+  const uint32_t n = L.n;
+  p->rank = rank;
+  p->world = world;
+  p->n = n;
+  p->V = L.V;
+  p->real = static_cast<uint32_t>((static_cast<uint64_t>(L.V) + world - 1 - rank) / world);
+  // local CSC: rows = this partition's vertices, sources as global ids
+  std::vector<uint64_t> off(static_cast<size_t>(n) + 1, 0);
+  std::vector<uint32_t> odeg(n, 0), ideg(n, 0);
+  const uint32_t lo = rank * n;
+  for (uint32_t v = 0; v < L.V; ++v) {
+    const uint32_t gv = L.gid[v];
+    if (gv >= lo && gv < lo + n) {
+      odeg[gv - lo] = L.outdeg[v];
+      ideg[gv - lo] = L.indeg[v];
+    }
+  }
+  for (uint32_t r = 0; r < n; ++r) off[r + 1] = off[r] + ideg[r];
+  std::vector<uint32_t> adj(off[n]);
+  std::vector<uint64_t> pos(off.begin(), off.end() - 1);
+  const uint64_t m = info->edges;
+  for (uint64_t i = 0; i < m; ++i) {
+    const uint32_t gs = L.gid[src[i]], gd = L.gid[dst[i]];
+    if (gd >= lo && gd < lo + n) adj[pos[gd - lo]++] = gs;
+    if (!info->is_directed && gs >= lo && gs < lo + n) adj[pos[gs - lo]++] = gd;
+  }
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int64_t r = 0; r < static_cast<int64_t>(n); ++r) std::sort(adj.begin() + off[r], adj.begin() + off[r + 1]);
+  plato_graph* g = new plato_graph();
+  p->g = g;
+  PLATO_CUDA_TRY(cudaGetDevice(&g->device));
+  g->info.is_directed = 1;
+  g->info.vertices = n;
+  g->info.edges = off[n];
+  g->info.max_v_i = n - 1;
+  g->stored_edges = off[n];
+  g->relabeled = true;  // rows sorted by descending in-degree: the binned pull plan applies
+  PLATO_TRY(g->in_off.alloc(static_cast<size_t>(n) + 1));
+  PLATO_TRY(g->in_adj.alloc(std::max<size_t>(adj.size(), 1)));
+  PLATO_TRY(g->out_deg.alloc(n));
+  PLATO_TRY(g->in_deg.alloc(n));
+  PLATO_CUDA_TRY(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+  PLATO_CUDA_TRY(cudaMemcpy(g->in_off.p, off.data(), off.size() * 8, cudaMemcpyHostToDevice));
+  if (!adj.empty()) PLATO_CUDA_TRY(cudaMemcpy(g->in_adj.p, adj.data(), adj.size() * 4, cudaMemcpyHostToDevice));
+  PLATO_CUDA_TRY(cudaMemcpy(g->out_deg.p, odeg.data(), odeg.size() * 4, cudaMemcpyHostToDevice));
+  PLATO_CUDA_TRY(cudaMemcpy(g->in_deg.p, ideg.data(), ideg.size() * 4, cudaMemcpyHostToDevice));
+  p->gid = std::move(L.gid);
+  PLATO_TRY(partition_prepare(g, g->stream));
+  PLATO_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  return PLATO_OK;
+}
+
+}  // namespace
+}  // namespace plato_b200
+
+extern "C" int plato_partition_create(const plato_graph_info* info, const plato_vid_t* src,
+                                      const plato_vid_t* dst, uint32_t rank, uint32_t world,
+                                      plato_partition** out) {
+  if (!info || !out || (info->edges > 0 && (!src || !dst)))
+    return set_error(PLATO_EINVAL, "plato_partition_create: null argument");
+  *out = nullptr;
+  if (info->vertices == 0 || world == 0 || rank >= world)
+    return set_error(PLATO_EINVAL, "plato_partition_create: need vertices > 0 and rank < world");
+  plato_partition* p = new (std::nothrow) plato_partition();
+  if (!p) return set_error(PLATO_ENOMEM, "plato_partition_create: host allocation failed");
+  int rc = PLATO_OK;
+  try {
+    rc = build_partition(info, src, dst, rank, world, p);
+  } catch (const std::bad_alloc&) {
+    rc = set_error(PLATO_ENOMEM, "plato_partition_create: host allocation failed");
+  }
+  if (rc != PLATO_OK) {
+    delete p;
+    return rc;
+  }
+  *out = p;
+  return PLATO_OK;
+}
+
+extern "C" int plato_partition_destroy(plato_partition* p) {
+  delete p;
+  return PLATO_OK;
+}
+
+extern "C" int plato_partition_info(const plato_partition* p, uint32_t* vertices, uint32_t* rows,
+                                    uint32_t* real_rows, uint64_t* edges) {
+  if (!p) return set_error(PLATO_EINVAL, "plato_partition_info: null partition");
+  if (vertices) *vertices = p->V;
+  if (rows) *rows = p->n;
+  if (real_rows) *real_rows = p->real;
+  if (edges) *edges = p->g->stored_edges;
+  return PLATO_OK;
+}
+
+extern "C" int plato_partition_pagerank_init(plato_partition* p, float* d_state, double damping, void* stream) {
+  if (!p || !d_state) return set_error(PLATO_EINVAL, "plato_partition_pagerank_init: null argument");
+  if (!(damping >= 0.0 && damping <= 1.0)) return set_error(PLATO_EINVAL, "damping must be in [0, 1]");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const float ghost = static_cast<float>((1.0 - damping) / p->V);
+  k_part_init<<<grid_for(p->n, 256), 256, 0, st>>>(p->g->out_deg.p, p->n, p->real, p->V, ghost,
+                                                   d_state + static_cast<size_t>(p->rank) * p->n);
+  PLATO_LAUNCHED("k_part_init");
+  return PLATO_OK;
+}
+
+extern "C" int plato_partition_pagerank_epoch(plato_partition* p, const float* d_state, float* d_next,
+                                              double damping, int final_epoch, double* d_delta, void* stream) {
+  if (!p || !d_state || !d_next) return set_error(PLATO_EINVAL, "plato_partition_pagerank_epoch: null argument");
+  if (!(damping >= 0.0 && damping <= 1.0)) return set_error(PLATO_EINVAL, "damping must be in [0, 1]");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t base = static_cast<size_t>(p->rank) * p->n;
+  return pull_epoch_partition(p->g, d_state, d_state + base, d_next + base,
+                              static_cast<float>((1.0 - damping) / p->V), static_cast<float>(damping),
+                              final_epoch != 0, st, d_delta);
+}
+
+extern "C" int plato_partition_ranks(const plato_partition* p, const float* h_state, float* ranks) {
+  if (!p || !h_state || !ranks) return set_error(PLATO_EINVAL, "plato_partition_ranks: null argument");
+  const std::vector<uint32_t>& gid = p->gid;
+#pragma omp parallel for schedule(static)
+  for (int64_t v = 0; v < static_cast<int64_t>(p->V); ++v) ranks[v] = h_state[gid[v]];
+  return PLATO_OK;
+}

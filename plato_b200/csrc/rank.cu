@@ -664,6 +664,27 @@ int with_host_output(plato_graph* g, float* host, F&& run) {
 }
 
 }  // namespace
+
+// 1D partitions (partition.cu): the workspace of a partition's rows, and one
+// PageRank pull epoch over them gathering the replicated state x_gather
+// (global ids) and updating the partition's slice (x_old -> xn); the sum of
+// the epoch's delta partials (normalised units) goes to *d_partial_sum.
+int partition_prepare(plato_graph* g, cudaStream_t st) { return ensure_ws(g, st); }
+
+int pull_epoch_partition(plato_graph* g, const float* x_gather, const float* x_old, float* xn, float tele,
+                         float d, bool final_epoch, cudaStream_t st, double* d_partial_sum) {
+  PLATO_TRY(ensure_ws(g, st));
+  const rank_update<teleport_uniform> upd{x_old, xn, g->out_deg.p, teleport_uniform{tele}, d,
+                                          final_epoch ? 1 : 0};
+  PLATO_TRY((pull_epoch_with<rank_update<teleport_uniform>, false>(g, x_gather, upd, nullptr, st)));
+  if (d_partial_sum) {
+    k_sum_partials<<<1, 1024, 0, st>>>(g->rank_ws->partials.p, static_cast<uint32_t>(partial_count(g)),
+                                       d_partial_sum);
+    PLATO_LAUNCHED("k_sum_partials");
+  }
+  return PLATO_OK;
+}
+
 }  // namespace plato_b200
 
 using namespace plato_b200;

@@ -1,0 +1,176 @@
+"""1D-partitioned PageRank over several GPUs (one process per GPU).
+
+The host side of ``plato_partition_*`` (include/plato_b200.h): every process
+builds its partition from the whole edge list, and each epoch is one pull
+over the partition's rows followed by an in-place all-gather of the next
+state over ``torch.distributed`` (NCCL over NVLink on GPUs), mirroring the
+reference's per-epoch exchange of pull messages (the reference sends each
+message to its owner over MPI, plato/graph/message_passing.hpp:88-144) and
+its delta allreduce (plato/graph/state/detail.hpp:77).
+
+    from plato_b200.partition import pagerank_partitioned
+    ranks, epochs = pagerank_partitioned(V, src, dst, iterations=20)   # inside torchrun
+
+``emulate_partitions`` runs P partitions in one process on one GPU, one after
+the other on a shared state buffer (each writes its own slice, so the
+assembled state needs no exchange): the partition kernels and layout with no
+collective, for checks on a single GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, load
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def layout(vertices: int, src, dst, world: int, is_directed: bool = True):
+    """-> (global internal id of every caller vertex, rows per partition); host only."""
+    lib = load()
+    s, d = _u32(src), _u32(dst)
+    info = _lib.GraphInfo(1 if is_directed else 0, int(vertices), int(s.size), max(int(vertices) - 1, 0))
+    gid = np.empty(int(vertices), np.uint32)
+    n = C.c_uint32()
+    check(lib.plato_partition_layout(C.byref(info), C.c_void_p(s.ctypes.data), C.c_void_p(d.ctypes.data), world,
+                                     C.c_void_p(gid.ctypes.data), C.byref(n)), "plato_partition_layout")
+    return gid, int(n.value)
+
+
+class Partition:
+    """Partition `rank` of `world` of a graph, resident on the current GPU."""
+
+    def __init__(self, vertices: int, src, dst, rank: int, world: int, is_directed: bool = True):
+        self._lib = load()
+        s, d = _u32(src), _u32(dst)
+        info = _lib.GraphInfo(1 if is_directed else 0, int(vertices), int(s.size), max(int(vertices) - 1, 0))
+        h = C.c_void_p()
+        check(self._lib.plato_partition_create(C.byref(info), C.c_void_p(s.ctypes.data), C.c_void_p(d.ctypes.data),
+                                               rank, world, C.byref(h)), "plato_partition_create")
+        self._h = h
+        self.rank, self.world = rank, world
+        v, n, real, e = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint64()
+        check(self._lib.plato_partition_info(h, C.byref(v), C.byref(n), C.byref(real), C.byref(e)),
+              "plato_partition_info")
+        self.vertices, self.rows, self.real_rows, self.edges = int(v.value), int(n.value), int(real.value), int(e.value)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.plato_partition_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init(self, d_state: int, damping: float, stream: int = 0):
+        check(self._lib.plato_partition_pagerank_init(self._h, C.c_void_p(d_state), damping, C.c_void_p(stream)),
+              "plato_partition_pagerank_init")
+
+    def epoch(self, d_state: int, d_next: int, damping: float, final: bool, d_delta: int | None = None,
+              stream: int = 0):
+        check(self._lib.plato_partition_pagerank_epoch(self._h, C.c_void_p(d_state), C.c_void_p(d_next), damping,
+                                                       1 if final else 0,
+                                                       C.c_void_p(d_delta) if d_delta else None,
+                                                       C.c_void_p(stream)), "plato_partition_pagerank_epoch")
+
+    def ranks(self, h_state: np.ndarray) -> np.ndarray:
+        """Caller-id ranks from the assembled state (host float32 [world * rows])."""
+        st = np.ascontiguousarray(h_state, dtype=np.float32)
+        out = np.empty(self.vertices, np.float32)
+        check(self._lib.plato_partition_ranks(self._h, C.c_void_p(st.ctypes.data), C.c_void_p(out.ctypes.data)),
+              "plato_partition_ranks")
+        return out
+
+
+def _epochs(step, iterations: int, eps: float, delta_of):
+    """The epoch schedule of pagerank.hpp:100-146: `step(final)` runs one
+    epoch; with eps > 0 a non-final epoch whose delta (reference units) is
+    below eps makes the next epoch the final one."""
+    epoch, ran = 0, 0
+    while epoch < iterations:
+        final = epoch == iterations - 1
+        step(final)
+        ran += 1
+        if not final and eps > 0.0 and delta_of() < eps:
+            epoch = iterations - 2
+        epoch += 1
+    return ran
+
+
+def pagerank_partitioned(vertices: int, src, dst, iterations: int = 100, damping: float = 0.85,
+                         eps: float = 0.0, is_directed: bool = True, group=None):
+    """PageRank over the processes of `group` (torch.distributed, default
+    group), one partition per process on its current GPU -> (caller-id ranks
+    float32 [V], epochs).  Every process passes the same edge list."""
+    import torch
+    import torch.distributed as dist
+
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    part = Partition(vertices, src, dst, rank, world, is_directed)
+    try:
+        n = part.rows
+        x = torch.empty(world * n, dtype=torch.float32, device="cuda")
+        xn = torch.empty_like(x)
+        delta = torch.zeros(1, dtype=torch.float64, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        part.init(x.data_ptr(), damping, stream)
+        dist.all_gather_into_tensor(x, x[rank * n:(rank + 1) * n], group=group)
+        bufs = [x, xn]
+
+        def step(final):
+            cur, nxt = bufs
+            part.epoch(cur.data_ptr(), nxt.data_ptr(), damping, final, delta.data_ptr() if eps > 0 else None, stream)
+            dist.all_gather_into_tensor(nxt, nxt[rank * n:(rank + 1) * n], group=group)
+            bufs.reverse()
+
+        def delta_of():
+            d = delta.clone()
+            dist.all_reduce(d, group=group)
+            return float(d.item()) * vertices
+
+        ran = _epochs(step, iterations, eps, delta_of)
+        return part.ranks(bufs[0].cpu().numpy()), ran
+    finally:
+        part.close()
+
+
+def emulate_partitions(vertices: int, src, dst, world: int, iterations: int = 100, damping: float = 0.85,
+                       eps: float = 0.0, is_directed: bool = True):
+    """The partitioned PageRank with `world` partitions on the current GPU in
+    one process -> (caller-id ranks float32 [V], epochs)."""
+    import torch
+
+    parts = [Partition(vertices, src, dst, r, world, is_directed) for r in range(world)]
+    try:
+        n = parts[0].rows
+        x = torch.empty(world * n, dtype=torch.float32, device="cuda")
+        xn = torch.empty_like(x)
+        deltas = torch.zeros(world, dtype=torch.float64, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        for p in parts:
+            p.init(x.data_ptr(), damping, stream)
+        bufs = [x, xn]
+
+        def step(final):
+            cur, nxt = bufs
+            for r, p in enumerate(parts):
+                p.epoch(cur.data_ptr(), nxt.data_ptr(), damping, final,
+                        deltas[r:].data_ptr() if eps > 0 else None, stream)
+            bufs.reverse()
+
+        def delta_of():
+            return float(deltas.sum().item()) * vertices
+
+        ran = _epochs(step, iterations, eps, delta_of)
+        return parts[0].ranks(bufs[0].cpu().numpy()), ran
+    finally:
+        for p in parts:
+            p.close()
