@@ -28,6 +28,11 @@ namespace plato_b200 {
 enum : uint8_t { COL_FREE = 0, COL_LIVE = 1, COL_FINAL = 2, COL_DONE = 3 };
 
 constexpr int kBatchTile = 2048;  // merge items per CTA (1024: 5-9% slower at RMAT s22-s24)
+// Row gathers in flight per lane and CTAs per SM of k_batch_pull: 4 at 5 CTAs
+// beat 8 at 4 (K = 64: 103.6 -> 100.9 ms per batch at RMAT s22; 6 or 8 at 5
+// CTAs spill and lose 7%).
+constexpr int kBatchInflight = 4;
+constexpr int kBatchMinBlocks = 5;
 
 struct seed_index_view {
   const uint32_t* off;   // [V+1] by internal vertex
@@ -160,7 +165,7 @@ __device__ __forceinline__ void merge_search(const uint32_t* s_rowend, int nrows
 }
 
 template <int GL, int VEC>
-__global__ void __launch_bounds__(256, 4) k_batch_pull(batch_pass p0) {
+__global__ void __launch_bounds__(256, kBatchMinBlocks) k_batch_pull(batch_pass p0) {
   constexpr int KT = GL * VEC, NG = 256 / GL, TILE = kBatchTile, IPG = TILE / NG;
   const batch_pass p = batch_tile_view<KT>(p0);
   __shared__ uint32_t s_rowend[TILE];
@@ -208,16 +213,16 @@ __global__ void __launch_bounds__(256, 4) k_batch_pull(batch_pass p0) {
   int jj = ja;
   for (int r = ra; r <= rb; ++r) {
     const int e_end = (r < rb) ? static_cast<int>(s_rowend[r]) : jb;
-    // rounds of eight row gathers in flight per lane; the last round of a
-    // row is predicated instead of a serial tail, so a row costs one gather
-    // latency per eight in-edges.  A lane whose columns are all finished or
-    // free loads nothing (its part of the row is never fetched), so a tile
-    // costs less as its columns converge.
-    for (; jj < e_end; jj += 8) {
+    // rounds of kBatchInflight row gathers in flight per lane; the last
+    // round of a row is predicated instead of a serial tail, so a row costs
+    // one gather latency per kBatchInflight in-edges.  A lane whose columns
+    // are all finished or free loads nothing (its part of the row is never
+    // fetched), so a tile costs less as its columns converge.
+    for (; jj < e_end; jj += kBatchInflight) {
       const int n = mine ? e_end - jj : 0;
-      float a[8][VEC];
+      float a[kBatchInflight][VEC];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
+      for (int u = 0; u < kBatchInflight; ++u) {
         if (u < n) {
           ldvec<VEC>(xl + static_cast<size_t>(s_src[jj + u]) * KT, a[u]);
         } else {
@@ -225,10 +230,9 @@ __global__ void __launch_bounds__(256, 4) k_batch_pull(batch_pass p0) {
           for (int c = 0; c < VEC; ++c) a[u][c] = 0.f;
         }
       }
+      static_assert(kBatchInflight == 4, "the row sum below adds four gathers");
 #pragma unroll
-      for (int c = 0; c < VEC; ++c)
-        acc[c] += ((a[0][c] + a[1][c]) + (a[2][c] + a[3][c])) +
-                  ((a[4][c] + a[5][c]) + (a[6][c] + a[7][c]));
+      for (int c = 0; c < VEC; ++c) acc[c] += (a[0][c] + a[1][c]) + (a[2][c] + a[3][c]);
     }
     jj = e_end;  // the last round may step past the row's end
     if (r < rb) {
