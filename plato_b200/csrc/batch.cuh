@@ -335,12 +335,15 @@ __global__ void __launch_bounds__(256) k_batch_fixup(batch_pass p0) {
 }
 
 // delta[q] = sum over rows of the column tile's partials[row][c] in row order;
-// grid (kt, column tiles), q = blockIdx.y * kt + blockIdx.x.
+// grid (kt, column tiles), q = blockIdx.y * kt + blockIdx.x.  Also clears the
+// live-column count that k_batch_states (the next launch) accumulates.
 static __global__ void __launch_bounds__(256) k_batch_delta(const double* __restrict__ partials,
                                                             uint32_t rows, uint32_t kt,
                                                             const uint8_t* __restrict__ state,
-                                                            double* __restrict__ delta) {
+                                                            double* __restrict__ delta,
+                                                            uint32_t* __restrict__ live_count) {
   __shared__ double s_red[32];
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *live_count = 0u;
   const uint32_t c = blockIdx.x;
   const uint32_t q = blockIdx.y * kt + c;
   if (state[q] != COL_LIVE) return;  // block-uniform

@@ -205,9 +205,9 @@ int batch_engine::launch_iteration(int parity) {
   p.thead = thead_.p;
   p.partials = partials_.p;
   const uint32_t T = mt.count;
-  // live count restarts every iteration; the retired list accumulates over
-  // the iterations of one step() and is reset there
-  PLATO_CUDA_TRY(cudaMemsetAsync(counters_.p, 0, sizeof(uint32_t), st_));
+  // the live count restarts every iteration (k_batch_delta clears it); the
+  // retired list accumulates over the iterations of one step() and is reset
+  // and read there
   const uint32_t fix_blocks = rows_ - T;
   switch (kt_) {
     case 8: PLATO_TRY((launch_pass<2, 4>(p, T, fix_blocks, ntiles_, st_))); break;
@@ -216,16 +216,13 @@ int batch_engine::launch_iteration(int parity) {
     case 64: PLATO_TRY((launch_pass<16, 4>(p, T, fix_blocks, ntiles_, st_))); break;
     default: PLATO_TRY((launch_pass<32, 4>(p, T, fix_blocks, ntiles_, st_))); break;
   }
-  k_batch_delta<<<dim3(kt_, ntiles_), 256, 0, st_>>>(partials_.p, rows_, kt_, state_.p, delta_.p);
+  k_batch_delta<<<dim3(kt_, ntiles_), 256, 0, st_>>>(partials_.p, rows_, kt_, state_.p, delta_.p,
+                                                     counters_.p);
   PLATO_LAUNCHED("k_batch_delta");
   k_batch_states<<<grid_for(Kp_, 256, 64), 256, 0, st_>>>(
       Kp_, state_.p, iters_.p, parity_.p, delta_.p, max_iterations_, eps_, parity ^ 1,
       counters_.p, retired_.p, counters_.p + 1);
   PLATO_LAUNCHED("k_batch_states");
-  PLATO_CUDA_TRY(cudaMemcpyAsync(h_counters_, counters_.p, 2 * sizeof(uint32_t),
-                                 cudaMemcpyDeviceToHost, st_));
-  PLATO_CUDA_TRY(cudaMemcpyAsync(h_counters_ + 2, retired_.p, Kp_ * sizeof(uint32_t),
-                                 cudaMemcpyDeviceToHost, st_));
   return PLATO_OK;
 }
 
@@ -365,6 +362,9 @@ int batch_engine::step(uint32_t* live, std::vector<uint32_t>* retired, uint32_t 
     count_launch(kKernelsPerIteration);
     cur_ ^= 1;
   }
+  // one read of the counters and the retired list per poll
+  PLATO_CUDA_TRY(cudaMemcpyAsync(h_counters_, counters_.p, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st_));
+  PLATO_CUDA_TRY(cudaMemcpyAsync(h_counters_ + 2, retired_.p, Kp_ * sizeof(uint32_t), cudaMemcpyDeviceToHost, st_));
   PLATO_CUDA_TRY(cudaStreamSynchronize(st_));
   *live = h_counters_[0];
   const uint32_t nret = std::min(h_counters_[1], Kp_);
@@ -449,6 +449,10 @@ int batch_engine::topk(const std::vector<uint32_t>& cols, uint32_t k, uint32_t* 
   k_topk_init<<<grid_for(n, 256), 256, 0, st_>>>(j, k);
   PLATO_LAUNCHED("k_topk_init");
   const unsigned blocks = 148 * 4;
+  // a column is usually bounded after two or three digits: the first two
+  // passes are enqueued without a host check (a finished column's lanes skip
+  // the next pass), later ones stop as soon as every column is bounded
+  constexpr int kUncheckedPasses = 2;
   for (int pass = 0; pass < 8; ++pass) {
     for (uint32_t c0 = 0; c0 < n; c0 += 32) {
       k_topk_hist<<<blocks, 256, 0, st_>>>(j, c0);
@@ -457,6 +461,7 @@ int batch_engine::topk(const std::vector<uint32_t>& cols, uint32_t k, uint32_t* 
     PLATO_CUDA_TRY(cudaMemsetAsync(undone.p, 0, sizeof(uint32_t), st_));
     k_topk_pick<<<grid_for(n, 256), 256, 0, st_>>>(j, k, undone.p);
     PLATO_LAUNCHED("k_topk_pick");
+    if (pass + 1 < kUncheckedPasses) continue;
     uint32_t h_undone = 0;
     PLATO_CUDA_TRY(cudaMemcpyAsync(&h_undone, undone.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st_));
     PLATO_CUDA_TRY(cudaStreamSynchronize(st_));
