@@ -33,8 +33,11 @@ REF_ROOT = Path(os.environ.get("PLATO_REFERENCE_ROOT", "/root/reference"))
 REF_SHIM = HERE / "hll_ref_shim.cpp"
 REF_LIB = HERE / "_ref" / "libhll_ref.so"
 PLATO_SHIM = HERE / "ref_shim" / "plato_ref_shim.cpp"
+PLATO_SHIM_W = HERE / "ref_shim" / "plato_ref_shim_weighted.cpp"
+PLATO_SHIM_H = HERE / "ref_shim" / "shim_common.hpp"
 PLATO_SHIM_INC = HERE / "ref_shim" / "include"
 PLATO_LIB = HERE / "_ref" / "libplato_ref.so"
+PLATO_LIB_W = HERE / "_ref" / "libplato_ref_weighted.so"
 
 
 def _newer(lib: Path, *deps: Path) -> bool:
@@ -46,9 +49,11 @@ def build_ref(force: bool = False, ref_root: Path = REF_ROOT) -> Path | None:
     where they lie in the reference tree:
       libhll_ref.so    hll_ref_shim.cpp over plato/util/hyperloglog.hpp +
                        hash.hpp (header-only, no dependencies);
-      libplato_ref.so  ref_shim/plato_ref_shim.cpp over the engine, graph and
+      libplato_ref.so, libplato_ref_weighted.so
+                       ref_shim/plato_ref_shim*.cpp over the engine, graph and
                        algorithm headers (pagerank, personalized_pagerank, bfs,
-                       trustrank), against the one-rank stand-ins in
+                       trustrank, weighted_pagerank, connected_component_t,
+                       hyperanf), against the one-rank stand-ins in
                        ref_shim/include for the libraries the reference needs.
     Returns None when the reference tree is absent (the committed golden
     vectors under tests/golden/ stand in)."""
@@ -63,16 +68,20 @@ def build_ref(force: bool = False, ref_root: Path = REF_ROOT) -> Path | None:
         os.replace(tmp, REF_LIB)
     if (ref_root / "plato" / "engine" / "dualmode.hpp").exists():
         stubs = [p for p in PLATO_SHIM_INC.rglob("*") if p.is_file()]
-        if force or not _newer(PLATO_LIB, PLATO_SHIM, *stubs):
-            tmp = PLATO_LIB.with_suffix(".so.tmp")
+        # one library per translation unit: the reference's headers define
+        # non-inline functions, so each of its programs is a single unit
+        for lib, src in ((PLATO_LIB, PLATO_SHIM), (PLATO_LIB_W, PLATO_SHIM_W)):
+            if not force and _newer(lib, src, PLATO_SHIM_H, *stubs):
+                continue
+            tmp = lib.with_suffix(".so.tmp")
             # the stand-ins come first on the include path; __DUALMODE_DEBUG__
             # makes the engine log its push/pull choice (dualmode.hpp:281-293)
             cmd = ["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-w", "-D__DUALMODE_DEBUG__",
                    "-I", str(PLATO_SHIM_INC), "-I", str(ref_root),
-                   "-I", str(ref_root / "plato" / "util" / "libcuckoo"),
-                   "-o", str(tmp), str(PLATO_SHIM), "-Wl,--no-undefined"]
+                   "-I", str(ref_root / "plato" / "util" / "libcuckoo"), "-I", str(PLATO_SHIM.parent),
+                   "-o", str(tmp), str(src), "-Wl,--no-undefined"]
             subprocess.run(cmd, check=True)
-            os.replace(tmp, PLATO_LIB)
+            os.replace(tmp, lib)
     return REF_LIB
 
 

@@ -356,6 +356,13 @@ inline int MPI_Allgatherv(const void* send, int scount, MPI_Datatype st, void* r
               static_cast<size_t>(scount) * plato_shim_mpi::type_size(st));
   return MPI_SUCCESS;
 }
+inline int MPI_Gatherv(const void* send, int scount, MPI_Datatype st, void* recv, const int*, const int* displs,
+                       MPI_Datatype rt, int, MPI_Comm) {
+  if (send == MPI_IN_PLACE) return MPI_SUCCESS;
+  std::memcpy(static_cast<char*>(recv) + static_cast<size_t>(displs[0]) * plato_shim_mpi::type_size(rt), send,
+              static_cast<size_t>(scount) * plato_shim_mpi::type_size(st));
+  return MPI_SUCCESS;
+}
 inline int MPI_Gather(const void* send, int scount, MPI_Datatype st, void* recv, int, MPI_Datatype, int,
                       MPI_Comm) {
   plato_shim_mpi::reduce_copy(send, recv, scount, st);

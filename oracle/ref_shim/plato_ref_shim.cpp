@@ -37,12 +37,21 @@
 #include "plato/algo/ppr/personalized_pagerank.hpp"
 #include "plato/algo/bfs/bfs.hpp"
 #include "plato/algo/trustrank/trustrank.hpp"
+#include "plato/algo/cgm/connected_component.hpp"
+#include "plato/algo/hyperanf/hyperanf.hpp"
+
+#include "shim_common.hpp"
 
 DEFINE_int32(threads, -1, "threads (the reference's --threads)");
 
 namespace plato {
 void install_oneshot_signal_handlers() {}
 }  // namespace plato
+
+namespace plato_ref_shim {
+std::mutex g_log_mu;
+std::vector<std::string> g_lines;
+}  // namespace plato_ref_shim
 
 namespace {
 
@@ -55,41 +64,8 @@ struct ref_graph {
   std::unique_ptr<dcsc_spec_t> dcsc;
 };
 
-// captured log lines of the current call
-std::mutex g_log_mu;
-std::vector<std::string> g_lines;
-
-void capture(int severity, const char* text) {
-  if (severity != 0) return;
-  std::lock_guard<std::mutex> lock(g_log_mu);
-  g_lines.emplace_back(text);
-}
-
-void start_capture() {
-  std::lock_guard<std::mutex> lock(g_log_mu);
-  g_lines.clear();
-  plato_shim_log_sink() = &capture;
-}
-
-std::vector<std::string> stop_capture() {
-  std::lock_guard<std::mutex> lock(g_log_mu);
-  plato_shim_log_sink() = nullptr;
-  return std::move(g_lines);
-}
-
-void init_once() {
-  static std::once_flag once;
-  std::call_once(once, [] {
-    int argc = 1;
-    static char name[] = "plato_ref_shim";
-    static char* args[] = {name, nullptr};
-    char** argv = args;
-    plato::cluster_info_t::get_instance().initialize(&argc, &argv);
-  });
-}
-
 // mode trace from the engine's debug lines: bit i set = call i ran push-mode
-uint64_t mode_trace(const std::vector<std::string>& lines, uint32_t* calls) {
+uint64_t mode_trace(const std::vector<std::string>& lines) {
   uint64_t trace = 0;
   uint32_t n = 0;
   for (const auto& l : lines) {
@@ -97,31 +73,12 @@ uint64_t mode_trace(const std::vector<std::string>& lines, uint32_t* calls) {
     if (l.find("push-mode") != std::string::npos && n < 64) trace |= 1ull << n;
     ++n;
   }
-  if (calls) *calls = n;
   return trace;
 }
 
-template <typename STATE>
-void copy_out(const STATE& st, uint32_t V, double* out) {
-  for (uint32_t v = 0; v < V; ++v) out[v] = st[v];
-}
-
-// "[epoch-i], delta: X, ..." lines of pagerank.hpp:141-144 and
-// personalized_pagerank.hpp:126-128, 267-269
-uint32_t epoch_deltas(const std::vector<std::string>& lines, double* deltas, uint32_t cap) {
-  uint32_t n = 0;
-  for (const auto& l : lines) {
-    int e = 0;
-    double d = 0.0;
-    if (std::sscanf(l.c_str(), "[epoch-%d], delta: %lf", &e, &d) == 2) {
-      if (deltas && n < cap) deltas[n] = d;
-      ++n;
-    }
-  }
-  return n;
-}
-
 }  // namespace
+
+using namespace plato_ref_shim;
 
 extern "C" {
 
@@ -299,8 +256,53 @@ __attribute__((visibility("default"))) uint64_t refp_bfs(void* h, uint32_t root,
     }
   }
   *epochs = n;
-  *trace = mode_trace(lines, nullptr);
+  *trace = mode_trace(lines);
   return visited;
+}
+
+// connected_component_t::compute + summary (connected_component.hpp:173-340):
+// labels [max_v_i + 1], component count, major label with its vertex and
+// edge counts.
+__attribute__((visibility("default"))) int refp_cc(void* h, uint32_t* labels, uint64_t* components,
+                                                   uint32_t* major_label, uint64_t* major_vertices,
+                                                   uint64_t* major_edges) {
+  auto* g = static_cast<ref_graph*>(h);
+  using engine_t = plato::dualmode_engine_t<dcsc_spec_t, bcsr_spec_t>;
+  engine_t engine(std::shared_ptr<dcsc_spec_t>(g->dcsc.get(), [](dcsc_spec_t*) {}),
+                  std::shared_ptr<bcsr_spec_t>(g->bcsr.get(), [](bcsr_spec_t*) {}), g->info);
+  plato::algo::connected_component_t<dcsc_spec_t, bcsr_spec_t> cc(&engine, g->info);
+  start_capture();
+  cc.compute();
+  stop_capture();
+  copy_out_u32(*cc.get_labels(), g->info.max_v_i_ + 1, labels);
+  *components = static_cast<uint64_t>(cc.get_num_components());
+  *major_label = cc.get_major_label();
+  *major_vertices = cc.get_major_vertices();
+  const auto* info = cc.get_components_info();
+  const auto it = info->find(cc.get_major_label());
+  *major_edges = it == info->end() ? 0 : it->second.edges_;
+  return 0;
+}
+
+// algo::hyperanf (hyperanf.hpp:83-195): the average distance, for register
+// widths 6 and 8 (the template argument).
+__attribute__((visibility("default"))) int refp_hyperanf(void* h, uint32_t bits, uint32_t iteration,
+                                                         double* avg_distance) {
+  auto* g = static_cast<ref_graph*>(h);
+  plato::algo::hyperanf_opts_t opts;
+  opts.iteration_ = iteration;
+  opts.bits = bits;
+  start_capture();
+  if (bits == 6)
+    *avg_distance = plato::algo::hyperanf<dcsc_spec_t, bcsr_spec_t, 6>(*g->dcsc, *g->bcsr, g->info, opts);
+  else if (bits == 8)
+    *avg_distance = plato::algo::hyperanf<dcsc_spec_t, bcsr_spec_t, 8>(*g->dcsc, *g->bcsr, g->info, opts);
+  else {
+    stop_capture();
+    return 1;
+  }
+  stop_capture();
+  return 0;
 }
 
 }  // extern "C"

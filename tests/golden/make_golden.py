@@ -19,7 +19,10 @@ lines skipped) and writes
                   compiled into oracle/_ref/libplato_ref.so by build_ref; see
                   oracle/refplato.py): ranks, epoch counts, per-epoch deltas,
                   BFS visited counts, vertices activated per level and the
-                  engine's push/pull choice per level.
+                  engine's push/pull choice per level; connected_component_t
+                  labels and summary and hyperanf average distances on the
+                  undirected graphs; weighted_pagerank on the weighted
+                  fixture and a weighted RMAT graph.
 The reference tree is only needed to regenerate; tests read the outputs.
 """
 from __future__ import annotations
@@ -199,7 +202,28 @@ def ref_vectors(root: Path) -> dict:
         for m in (0, 1):
             r, ep = g.trustrank(good, 20, m, 100, 0.85, 0.001)
             out[f"{name}__tr_m{m}"], out[f"{name}__tr_m{m}_epochs"] = r, ep
+        if not directed:  # connected_component_t and hyperanf run on undirected graphs
+            lab, comps, major, mv, me = g.connected_components()
+            out[f"{name}__cc_labels"] = lab
+            out[f"{name}__cc_summary"] = np.array([comps, major, mv, me], np.uint64)
+            out[f"{name}__anf_avg"] = np.array([g.hyperanf(6, 20), g.hyperanf(8, 20)])
         g.close()
+    # weighted PageRank: the reference's weighted fixture and a weighted RMAT s12
+    from oracle.refplato import WeightedReferenceGraph
+    z = np.load(HERE / "fixtures.npz")
+    for name, (s, d, w) in {"w10": (z["raw_graph_10_9_weighted__src"], z["raw_graph_10_9_weighted__dst"],
+                                    z["raw_graph_10_9_weighted__w"]),
+                            "wrmat12": ref_graph_edges(root, (12, 1, False)) + (None,)}.items():
+        if w is None:  # seeded weights, exactly representable as float32 (stored that way)
+            w32 = np.random.default_rng(12).uniform(0.1, 10.0, s.size).astype(np.float32)
+            out[f"{name}__w"] = w32
+            w = w32.astype(np.float64)
+        V = int(max(s.max(), d.max())) + 1
+        wg = WeightedReferenceGraph(V, s, d, w, True)
+        for tag, eps in (("100", 0.0), ("eps", 0.001)):
+            r, ep = wg.weighted_pagerank(100, 0.85, eps)
+            out[f"{name}__wpr{tag}"], out[f"{name}__wpr{tag}_epochs"] = r, ep
+        wg.close()
     return {k: np.asarray(v) for k, v in out.items()}
 
 

@@ -123,3 +123,39 @@ def test_oracle_matches_reference_live_rmat16(directed):
     finally:
         ref.close()
         g.close()
+
+
+@pytest.mark.parametrize("name", ["v100u", "rmat12u"])
+def test_oracle_cc_and_hyperanf_match_reference(gold, name):
+    """connected_component_t labels (the fixed point: each component's
+    smallest id) and hyperanf's average distance at register widths 6 and 8."""
+    from oracle import fp64, hll
+    V = int(gold[f"{name}__meta"][0])
+    s, d = graph_edges(name)
+    np.testing.assert_array_equal(fp64.cc_labels(V, s, d, False), gold[f"{name}__cc_labels"])
+    comps, major, mv, _ = (int(x) for x in gold[f"{name}__cc_summary"])
+    lab = gold[f"{name}__cc_labels"]
+    vals, counts = np.unique(lab, return_counts=True)
+    assert vals.size == comps and (lab == major).sum() == mv == counts.max()
+    for bits, want in zip((6, 8), gold[f"{name}__anf_avg"]):
+        avg, _, _, _ = hll.hyperanf(V, s, d, False, bits, 20)
+        assert avg == pytest.approx(float(want), rel=1e-12), bits
+
+
+def weighted_edges(gold, name):
+    if name == "w10":
+        z = np.load(FIXTURES)
+        return z["raw_graph_10_9_weighted__src"], z["raw_graph_10_9_weighted__dst"], z["raw_graph_10_9_weighted__w"]
+    _, s, d = oracle.rmat(12, 16, 1)
+    return s, d, gold["wrmat12__w"].astype(np.float64)
+
+
+@pytest.mark.parametrize("name", ["w10", "wrmat12"])
+def test_oracle_weighted_pagerank_matches_reference(gold, name):
+    from oracle import fp64
+    s, d, w = weighted_edges(gold, name)
+    V = int(max(s.max(), d.max())) + 1
+    for tag, eps in (("100", 0.0), ("eps", 0.001)):
+        r, ep, _ = fp64.weighted_pagerank(V, s, d, w, True, 100, 0.85, eps)
+        assert ep == int(gold[f"{name}__wpr{tag}_epochs"]), tag
+        assert close(r, gold[f"{name}__wpr{tag}"]), tag

@@ -67,3 +67,32 @@ def test_gpu_matches_reference_outputs(gold, name):
             r, _, st = g.trustrank(good, 100, 0.85, 20, m, 0.001)
             assert abs(st.iterations - int(gold[f"{name}__tr_m{m}_epochs"])) <= 1, m
             assert l1(r, gold[f"{name}__tr_m{m}"]) <= L1_TOL, m
+
+
+@pytest.mark.parametrize("name", ["v100u", "rmat12u"])
+def test_gpu_cc_and_hyperanf_match_reference(gold, name):
+    V = int(gold[f"{name}__meta"][0])
+    s, d = graph_edges(name)
+    with pb.Graph(V, s, d, False) as g:
+        lab, summ, _ = g.connected_components()
+        np.testing.assert_array_equal(lab, gold[f"{name}__cc_labels"])
+        comps, major, mv, me = (int(x) for x in gold[f"{name}__cc_summary"])
+        assert summ["components"] == comps and summ["major_label"] == major
+        assert summ["major_vertices"] == mv
+        for bits, want in zip((6, 8), gold[f"{name}__anf_avg"]):
+            avg, _, _, _ = g.hyperanf(20, bits)
+            assert avg == pytest.approx(float(want), rel=1e-12), bits
+
+
+@pytest.mark.parametrize("name", ["w10", "wrmat12"])
+def test_gpu_weighted_pagerank_matches_reference(gold, name):
+    from tests.test_cpu_reference_pin import weighted_edges
+    s, d, w = weighted_edges(gold, name)
+    V = int(max(s.max(), d.max())) + 1
+    with pb.Graph(V, s, d, True, weights=w) as g:
+        for tag, eps in (("100", 0.0), ("eps", 0.001)):
+            r, st = g.weighted_pagerank(100, 0.85, eps)
+            want = gold[f"{name}__wpr{tag}"]
+            assert abs(st.iterations - int(gold[f"{name}__wpr{tag}_epochs"])) <= 1, tag
+            # the reference's units (ranks sum to ~V): L1 / V within the PageRank tolerance
+            assert l1(r, want) / V <= L1_TOL, tag
