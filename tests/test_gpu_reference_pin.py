@@ -78,7 +78,7 @@ def test_gpu_cc_and_hyperanf_match_reference(gold, name):
         np.testing.assert_array_equal(lab, gold[f"{name}__cc_labels"])
         comps, major, mv, me = (int(x) for x in gold[f"{name}__cc_summary"])
         assert summ["components"] == comps and summ["major_label"] == major
-        assert summ["major_vertices"] == mv
+        assert summ["major_vertices"] == mv and summ["major_edges"] == me
         for bits, want in zip((6, 8), gold[f"{name}__anf_avg"]):
             avg, _, _, _ = g.hyperanf(20, bits)
             assert avg == pytest.approx(float(want), rel=1e-12), bits
