@@ -724,16 +724,16 @@ def suite_ppr_single(pb):
 def suite_batch(pb, plain_n=16, quick=False):
     """Batched multi-source PPR on RMAT s22 seed 4 (K in 64/256/1024, Zipf seed
     sets 1..32, eps 1e-6) against the plain engine running the same queries one
-    at a time (plato_seedset_ppr, pull-only).  quick: one K=256 batch only (for
+    at a time (plato_seedset_ppr, pull-only).  quick: one K=128 batch only (for
     profiler captures)."""
     V, s, d = pb.rmat(22, 16, 4)
     g = pb.Graph(V, s, d, is_directed=True)
     deg = np.bincount(s, minlength=V)
     sets = zipf_seed_sets(deg, 1024, 32, 4)
-    if quick:
-        out = g.ppr_batch(sets[:256], 300, 0.85, 1e-6, topk=100)
+    if quick:  # one K = 128 batch at k_tile 128, no autotuning: about 3 GB on the device
+        out = g.ppr_batch(sets[:128], 300, 0.85, 1e-6, topk=100, k_tile=128)
         g.close()
-        return {"workload": "ppr_batch_rmat_s22_ef16_seed4", "K": 256,
+        return {"workload": "ppr_batch_rmat_s22_ef16_seed4", "K": 128, "k_tile": 128,
                 "iterations_max": int(out["iterations"].max())}
     g.seedset_ppr(sets[0], 300, 0.85, 1e-6)
     t0 = time.perf_counter()
@@ -870,8 +870,42 @@ def run_ceiling(args):
                           "frac": bins["k_pull_long"] / (tot / n / 1e3) / 1e9 / peak}
     out["peak"] = {"hbm_gbs": peak, "source": kind}
     g.close()
+    out["batch"] = {"s22": batch_ceiling(pb, 22, 4), "s24": batch_ceiling(pb, 24, 5)}
     print(json.dumps(out), flush=True)
     return 0
+
+
+BATCH_CEILING_MODES = ["rows", "sequential_rows", "l2_rows", "k_batch_iteration"]
+
+
+def batch_ceiling(pb, scale, seed, kts=(64, 128), reps=5):
+    """The batched pull's row-gather stream on the batched / serving graph
+    (plato_diag_batch_ceiling modes 0-2) beside the real batched iteration
+    (mode 3) at the same tile widths.  Times are CUDA-event averages."""
+    import ctypes as C
+
+    from plato_b200 import _lib
+    lib = _lib.load()
+    V, s, d = pb.rmat(scale, 16, seed)
+    g = pb.Graph(V, s, d, is_directed=True)
+    E = int(s.size)
+    del s, d
+    peak, kind = measured_peak()
+    out = {"workload": f"rmat_s{scale}_ef16_seed{seed}", "vertices": V, "edges": E,
+           "peak": {"hbm_gbs": peak, "source": kind}}
+    for kt in kts:
+        row = {}
+        for mode, name in enumerate(BATCH_CEILING_MODES):
+            ms, n, cs = C.c_double(), C.c_uint64(), C.c_double()
+            _lib.check(lib.plato_diag_batch_ceiling(g.handle, kt, mode, reps, C.byref(ms), C.byref(n), C.byref(cs)),
+                       "plato_diag_batch_ceiling")
+            # bytes the stream needs: ids + one kt-float row per edge
+            b = 4 * E + 4 * E * kt
+            row[name] = {"ms": ms.value, "row_bytes_gbs": b / (ms.value / 1e3) / 1e9,
+                         "frac": b / (ms.value / 1e3) / 1e9 / peak}
+        out[f"kt{kt}"] = row
+    g.close()
+    return out
 
 
 def run_suite(args):

@@ -358,6 +358,17 @@ int plato_partition_ranks(const plato_partition* p, const float* h_state, float*
  * paths. */
 int plato_diag_pull_ceiling(plato_graph* g, uint32_t mode, uint32_t reps, double* ms_per_launch,
                             uint64_t* edges, double* checksum);
+/* No counterpart in the reference.  The batched PPR pull's row-gather stream
+ * at column-tile width kt (16/32/64/128): every CSC edge gathers its source's
+ * kt-float row (a float4 per lane, 4 rows in flight per lane, as the batched
+ * pull), with the row sums, update and delta taken out: mode 0 the real
+ * source rows; 1 rows at the edge position mod V (sequential rows); 2 sources
+ * folded into the first 16 MB of rows (L2-resident).  Mode 3 times the real
+ * batched iteration over kt live columns that never converge.  Same outputs
+ * and caveats as plato_diag_pull_ceiling (*edges = all stored edges); any
+ * vertex order. */
+int plato_diag_batch_ceiling(plato_graph* g, uint32_t kt, uint32_t mode, uint32_t reps, double* ms_per_launch,
+                             uint64_t* edges, double* checksum);
 
 /* ---- batched multi-source personalized pagerank --------------------------
  * K queries, query q's seed set is seeds[seed_offsets[q] .. seed_offsets[q+1]).

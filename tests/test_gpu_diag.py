@@ -30,3 +30,27 @@ def test_ceiling_modes_run_and_count_their_gathers():
         assert lib.plato_diag_pull_ceiling(g.handle, 6, 4, C.byref(ms), None, None) == _lib.PLATO_EINVAL
     with pb.Graph(V, s, d, True, relabel=False) as g:
         assert lib.plato_diag_pull_ceiling(g.handle, 1, 4, C.byref(ms), None, None) == _lib.PLATO_EINVAL
+
+
+@pytest.mark.parametrize("kt", [16, 128])
+def test_batch_ceiling_modes_run_and_count_their_gathers(kt):
+    """plato_diag_batch_ceiling: every row of its state sums to 1, so the
+    checksum of modes 0-2 is (3 warm-ups + 4 timed) x the stored edges; mode 3
+    runs the real batched iteration and reports its live columns."""
+    lib = _lib.load()
+    V, s, d = pb.rmat(14, 16, 9)
+    for relabel in (True, False):
+        with pb.Graph(V, s, d, True, relabel=relabel) as g:
+            E = g.device_view().stored_edges
+            for mode in range(4):
+                ms, n, cs = C.c_double(), C.c_uint64(), C.c_double()
+                _lib.check(lib.plato_diag_batch_ceiling(g.handle, kt, mode, 4, C.byref(ms), C.byref(n),
+                                                        C.byref(cs)), "plato_diag_batch_ceiling")
+                assert n.value == E and ms.value > 0
+                if mode < 3:
+                    assert cs.value == pytest.approx(7 * E, rel=1e-4)
+                else:
+                    assert cs.value == kt
+            ms = C.c_double()
+            assert lib.plato_diag_batch_ceiling(g.handle, kt, 4, 4, C.byref(ms), None, None) == _lib.PLATO_EINVAL
+            assert lib.plato_diag_batch_ceiling(g.handle, 8, 0, 4, C.byref(ms), None, None) == _lib.PLATO_EINVAL
