@@ -114,6 +114,10 @@ __device__ __forceinline__ void batch_finalize(const batch_pass& p, uint32_t v,
                                                const float (&y)[VEC], const uint8_t (&st)[VEC],
                                                int lane_g, float (&dl)[VEC]) {
   constexpr int KT = GL * VEC;
+  bool running = false;
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) running |= (st[c] == COL_LIVE || st[c] == COL_FINAL);
+  if (!running) return;  // nothing of this lane's columns is read or written
   float tele[VEC];
 #pragma unroll
   for (int c = 0; c < VEC; ++c) tele[c] = 0.f;
@@ -126,8 +130,16 @@ __device__ __forceinline__ void batch_finalize(const batch_pass& p, uint32_t v,
   }
   const uint32_t dg = p.deg[v];
   const size_t base = static_cast<size_t>(v) * KT + lane_g * VEC;
+  bool live = false;
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) live |= (st[c] == COL_LIVE);
   float old[VEC];
-  ldvec_cs<VEC>(p.X + base, old);
+  if (live) {  // only a live column's delta needs its old value
+    ldvec_cs<VEC>(p.X + base, old);
+  } else {
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) old[c] = 0.f;
+  }
 #pragma unroll
   for (int c = 0; c < VEC; ++c) {
     const float r = fmaf(p.d, y[c], tele[c]);
