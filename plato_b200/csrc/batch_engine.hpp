@@ -52,6 +52,7 @@ class batch_engine {
   cudaStream_t st_ = nullptr;
   uint32_t K_ = 0, Kp_ = 0, kt_ = 0, ntiles_ = 0, rows_ = 0;
   uint32_t max_iterations_ = 0;
+  uint64_t hot_l2_bytes_ = 0;  // L2 bytes of hot rows the row gathers keep (half of L2)
   double eps_ = 0.0, damping_ = 0.85;
   int cur_ = 0;
   dbuf<float> X_[2];

@@ -30,6 +30,18 @@
 namespace plato_b200 {
 namespace {
 
+// Two timing events, destroyed on every way out.
+struct event_pair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  event_pair() = default;
+  event_pair(const event_pair&) = delete;
+  event_pair& operator=(const event_pair&) = delete;
+  ~event_pair() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
 __global__ void __launch_bounds__(256, 8) k_ceil_ids(const uint32_t* __restrict__ adj, uint64_t n,
                                                      uint32_t* __restrict__ sink) {
   const uint64_t n4 = n / 4;
@@ -73,15 +85,20 @@ __global__ void __launch_bounds__(256, (M <= 8 ? 8 : 4)) k_ceil_gather(const uin
 
 // Batched-pull row gathers: a group of GL lanes takes 4 consecutive edges of
 // the whole CSC id stream at a time and gathers the source's kt-float row
-// (kt = 4 GL, a float4 per lane, 4 rows in flight per lane, as k_batch_pull).
+// (kt = 4 GL, a float4 per lane, 4 rows in flight per lane, rows at or past
+// keep_rows loaded evict-first in L2, as k_batch_pull).
 // kMode: 0 the edge's own source row, 1 row = edge position mod V (sequential
 // rows: the streaming rate of the same instruction mix), 2 source folded into
 // the first hot_rows rows (an L2-resident block).
 template <int GL, int kMode>
 __global__ void __launch_bounds__(256, 5) k_ceil_rows(const uint32_t* __restrict__ adj, uint64_t n,
                                                       const float* __restrict__ X, uint32_t V,
-                                                      uint32_t hot_rows, float* __restrict__ sink) {
+                                                      uint32_t hot_rows, uint32_t keep_rows,
+                                                      float* __restrict__ sink) {
   constexpr int KT = GL * 4;
+  uint64_t pol_keep, pol_cold;
+  asm("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(pol_keep));
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol_cold));
   const unsigned lane_g = threadIdx.x % GL;
   const uint64_t groups = (uint64_t)gridDim.x * (blockDim.x / GL);
   float s = 0.f;
@@ -98,9 +115,13 @@ __global__ void __launch_bounds__(256, 5) k_ceil_rows(const uint32_t* __restrict
     }
     float4 a[4];
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
-      a[u] = (e0 + u < n) ? __ldg(reinterpret_cast<const float4*>(X + static_cast<size_t>(row[u]) * KT) + lane_g)
-                          : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int u = 0; u < 4; ++u) {
+      a[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (e0 + u < n)
+        asm("ld.global.nc.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+            : "=f"(a[u].x), "=f"(a[u].y), "=f"(a[u].z), "=f"(a[u].w)
+            : "l"(X + static_cast<size_t>(row[u]) * KT + 4 * lane_g), "l"(row[u] < keep_rows ? pol_keep : pol_cold));
+    }
 #pragma unroll
     for (int u = 0; u < 4; ++u) s += (a[u].x + a[u].y) + (a[u].z + a[u].w);
   }
@@ -115,11 +136,11 @@ __global__ void k_ceil_fill(float* X, uint64_t n, float v) {
 
 template <int GL>
 void launch_ceil_rows(uint32_t mode, unsigned grid, cudaStream_t st, const uint32_t* adj, uint64_t n,
-                      const float* X, uint32_t V, uint32_t hot_rows, float* sink) {
+                      const float* X, uint32_t V, uint32_t hot_rows, uint32_t keep_rows, float* sink) {
   switch (mode) {
-    case 0: k_ceil_rows<GL, 0><<<grid, 256, 0, st>>>(adj, n, X, V, hot_rows, sink); break;
-    case 1: k_ceil_rows<GL, 1><<<grid, 256, 0, st>>>(adj, n, X, V, hot_rows, sink); break;
-    default: k_ceil_rows<GL, 2><<<grid, 256, 0, st>>>(adj, n, X, V, hot_rows, sink); break;
+    case 0: k_ceil_rows<GL, 0><<<grid, 256, 0, st>>>(adj, n, X, V, hot_rows, keep_rows, sink); break;
+    case 1: k_ceil_rows<GL, 1><<<grid, 256, 0, st>>>(adj, n, X, V, hot_rows, keep_rows, sink); break;
+    default: k_ceil_rows<GL, 2><<<grid, 256, 0, st>>>(adj, n, X, V, hot_rows, keep_rows, sink); break;
   }
 }
 
@@ -172,17 +193,16 @@ extern "C" int plato_diag_pull_ceiling(plato_graph* g, uint32_t mode, uint32_t r
       count_launch();
     };
     for (int w = 0; w < 3; ++w) launch();
-    cudaEvent_t e0, e1;
-    PLATO_CUDA_TRY(cudaEventCreate(&e0));
-    PLATO_CUDA_TRY(cudaEventCreate(&e1));
+    event_pair ev;
+    PLATO_CUDA_TRY(cudaEventCreate(&ev.a));
+    PLATO_CUDA_TRY(cudaEventCreate(&ev.b));
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
     PLATO_CUDA_TRY(cudaEventRecord(e0, st));
     for (uint32_t r = 0; r < reps; ++r) launch();
     PLATO_CUDA_TRY(cudaEventRecord(e1, st));
     PLATO_CUDA_TRY(cudaEventSynchronize(e1));
     float ms = 0.f;
     PLATO_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     PLATO_CUDA_TRY(cudaGetLastError());
     *ms_per_launch = static_cast<double>(ms) / reps;
     if (checksum) {
@@ -213,9 +233,10 @@ extern "C" int plato_diag_batch_ceiling(plato_graph* g, uint32_t kt, uint32_t mo
     const uint64_t n = g->stored_edges;
     cudaStream_t st = g->stream;
     if (edges) *edges = n;
-    cudaEvent_t e0, e1;
-    PLATO_CUDA_TRY(cudaEventCreate(&e0));
-    PLATO_CUDA_TRY(cudaEventCreate(&e1));
+    event_pair ev;
+    PLATO_CUDA_TRY(cudaEventCreate(&ev.a));
+    PLATO_CUDA_TRY(cudaEventCreate(&ev.b));
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
     float ms = 0.f;
     double cs = 0.0;
     if (mode == 3) {
@@ -242,6 +263,11 @@ extern "C" int plato_diag_batch_ceiling(plato_graph* g, uint32_t kt, uint32_t mo
       const unsigned grid = 5u * static_cast<unsigned>(sms);
       // an L2-resident block of rows for mode 2: 16 MB
       const uint32_t hot_rows = std::max(1u, std::min(V, static_cast<uint32_t>((16u << 20) / (4u * kt))));
+      // the batched pull's L2 split: rows within half of L2 keep normal priority
+      int l2 = 0;
+      PLATO_CUDA_TRY(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, g->device));
+      const uint32_t keep_rows = static_cast<uint32_t>(
+          std::min<uint64_t>(V, static_cast<uint64_t>(l2) / 2 / (4ull * kt)));
       dbuf<float> X, sink;
       PLATO_TRY(X.alloc(static_cast<size_t>(V) * kt));
       PLATO_TRY(sink.alloc(grid));
@@ -252,10 +278,10 @@ extern "C" int plato_diag_batch_ceiling(plato_graph* g, uint32_t kt, uint32_t mo
       PLATO_CUDA_TRY(cudaMemsetAsync(sink.p, 0, 4ull * grid, st));
       auto launch = [&]() {
         switch (kt) {
-          case 16: launch_ceil_rows<4>(mode, grid, st, g->in_adj.p, n, X.p, V, hot_rows, sink.p); break;
-          case 32: launch_ceil_rows<8>(mode, grid, st, g->in_adj.p, n, X.p, V, hot_rows, sink.p); break;
-          case 64: launch_ceil_rows<16>(mode, grid, st, g->in_adj.p, n, X.p, V, hot_rows, sink.p); break;
-          default: launch_ceil_rows<32>(mode, grid, st, g->in_adj.p, n, X.p, V, hot_rows, sink.p); break;
+          case 16: launch_ceil_rows<4>(mode, grid, st, g->in_adj.p, n, X.p, V, hot_rows, keep_rows, sink.p); break;
+          case 32: launch_ceil_rows<8>(mode, grid, st, g->in_adj.p, n, X.p, V, hot_rows, keep_rows, sink.p); break;
+          case 64: launch_ceil_rows<16>(mode, grid, st, g->in_adj.p, n, X.p, V, hot_rows, keep_rows, sink.p); break;
+          default: launch_ceil_rows<32>(mode, grid, st, g->in_adj.p, n, X.p, V, hot_rows, keep_rows, sink.p); break;
         }
         count_launch();
       };
@@ -269,8 +295,6 @@ extern "C" int plato_diag_batch_ceiling(plato_graph* g, uint32_t kt, uint32_t mo
       PLATO_CUDA_TRY(cudaMemcpy(h.data(), sink.p, 4ull * grid, cudaMemcpyDeviceToHost));
       for (float v : h) cs += v;
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     PLATO_CUDA_TRY(cudaGetLastError());
     *ms_per_launch = static_cast<double>(ms) / reps;
     if (checksum) *checksum = cs;

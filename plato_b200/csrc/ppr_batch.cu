@@ -141,6 +141,11 @@ int batch_engine::init(uint32_t K, uint32_t kt, uint32_t max_iterations, double 
   damping_ = damping;
   eps_ = eps;
   const uint32_t V = g_->info.vertices;
+  if (hot_l2_bytes_ == 0) {
+    int l2 = 0;
+    PLATO_CUDA_TRY(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, g_->device));
+    hot_l2_bytes_ = static_cast<uint64_t>(l2) / 2;
+  }
   const merge_tiles* mt = nullptr;
   PLATO_TRY(ensure_pull_tiles(g_, kBatchTile, st_, &mt));
   const uint32_t T = mt->count;
@@ -209,6 +214,9 @@ int batch_engine::launch_iteration(int parity) {
   // retired list accumulates over the iterations of one step() and is reset
   // and read there
   const uint32_t fix_blocks = rows_ - T;
+  // rows whose gathers keep normal L2 priority: half of L2 for one column tile
+  // (a launch's CTAs run tile by tile, blockIdx.x fastest)
+  p.hot_rows = static_cast<uint32_t>(std::min<uint64_t>(V, hot_l2_bytes_ / (4ull * kt_)));
   switch (kt_) {
     case 8: PLATO_TRY((launch_pass<2, 4>(p, T, fix_blocks, ntiles_, st_))); break;
     case 16: PLATO_TRY((launch_pass<4, 4>(p, T, fix_blocks, ntiles_, st_))); break;
