@@ -63,33 +63,43 @@ class ClockSampler:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, period_ms: int = 50):
         self.gpu = gpu_index
+        self.period_ms = period_ms
         self.rows = []
-        self._stop = threading.Event()
+        self._proc = None
         self._t = None
 
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True,
-                                     text=True, timeout=5).stdout.strip()
-                if out:
-                    self.rows.append([c.strip() for c in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+    def _read(self):
+        for line in self._proc.stdout:
+            line = line.strip()
+            if line:
+                self.rows.append([c.strip() for c in line.split(",")])
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
+        # one nvidia-smi in loop mode (a sample every period_ms), stopped by its handle on exit
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                           "--format=csv,noheader,nounits", "-lms", str(self.period_ms)],
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self._proc = None
+            return self
+        self._t = threading.Thread(target=self._read, daemon=True)
         self._t.start()
         return self
 
     def __exit__(self, *exc):
-        self._stop.set()
+        # no wait on either side: an idle GPU lowers its clocks, and a sample
+        # taken then would not describe the timed region
+        if self._proc:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
         if self._t:
-            self._t.join(timeout=10)
+            self._t.join(timeout=5)
 
     def summary(self):
         if not self.rows:
