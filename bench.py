@@ -861,6 +861,24 @@ def suite_serving(pb, rates=(100, 1000, 5000, 20000), n_req=400, slot_options=(6
     return out
 
 
+def steady_window(t_done, lat_ms, slots):
+    """Steady-state rate of a serving run: t_done = completion times in
+    completion order, lat_ms = their latencies.  The first and last
+    h = min(slots, n / 4) completions are dropped (ramp-up and drain); the
+    rate is the n - 2h completions in between over the time they took, with
+    their latency percentiles.  A saturated server turns its slots over in
+    generations of `slots`, so h = slots spans whole generations."""
+    t_done = np.asarray(t_done, dtype=np.float64)
+    lat_ms = np.asarray(lat_ms, dtype=np.float64)
+    n = t_done.size
+    h = max(1, min(slots, n // 4))
+    w0, w1 = float(t_done[h - 1]), float(t_done[n - h - 1])
+    mid = lat_ms[h:n - h]
+    return {"dropped_each_end": h, "completions": n - 2 * h, "window_s": w1 - w0,
+            "qps": float((n - 2 * h) / (w1 - w0)) if w1 > w0 else None,
+            "p50_ms": float(np.percentile(mid, 50)), "p99_ms": float(np.percentile(mid, 99))}
+
+
 def _serve(pb, g, sets, rates, n_req, slots):
     """Drives a PPRServer with Poisson arrivals at each offered rate.  n_req:
     requests per rate (an int, or a function of the rate).  Besides the whole
@@ -902,12 +920,7 @@ def _serve(pb, g, sets, rates, n_req, slots):
             entry = {"offered_qps": rate, "requests": n, "sustained_qps": n / wall,
                      "p50_ms": float(np.percentile(lat_ms, 50)),
                      "p99_ms": float(np.percentile(lat_ms, 99))}
-            h = min(slots, n // 4)
-            w0, w1 = float(t_done[h - 1]), float(t_done[n - h - 1])
-            mid = lat_ms[h:n - h]
-            entry["steady"] = {"dropped_each_end": h, "completions": n - 2 * h, "window_s": w1 - w0,
-                               "qps": float((n - 2 * h) / (w1 - w0)) if w1 > w0 else None,
-                               "p50_ms": float(np.percentile(mid, 50)), "p99_ms": float(np.percentile(mid, 99))}
+            entry["steady"] = steady_window(t_done, lat_ms, slots)
             out[f"rate{rate}"] = entry
     return out
 
