@@ -829,13 +829,7 @@ def suite_batch(pb, plain_n=16, quick=False):
         g.close()
         return {"workload": "ppr_batch_rmat_s22_ef16_seed4", "K": 128, "k_tile": 128,
                 "iterations_max": int(out["iterations"].max())}
-    g.seedset_ppr(sets[0], 300, 0.85, 1e-6)
-    t0 = time.perf_counter()
-    plain_ranks = []
-    for q in range(plain_n):
-        r, _ = g.seedset_ppr(sets[q], 300, 0.85, 1e-6)
-        plain_ranks.append(r)
-    plain_qps = plain_n / (time.perf_counter() - t0)
+    plain_qps, _, plain_ranks = plain_engine_qps(g, sets, plain_n, collect=True)
     res = {"workload": "ppr_batch_rmat_s22_ef16_seed4", "vertices": V, "edges": int(s.size),
            "plain_qps": plain_qps, "plain_sample": plain_n}
     for K in (64, 256, 1024):
@@ -885,12 +879,8 @@ def suite_serving(pb, rates=(100, 1000, 5000, 20000), n_req=400, slot_options=(6
     deg = np.bincount(s, minlength=V)
     out = {"workload": "ppr_serving_rmat_s24_ef16_seed5", "vertices": V}
     sets = zipf_seed_sets(deg, n_req, 64, 5)
-    # plain engine, one query at a time
-    g.seedset_ppr(sets[0], 300, 0.85, 1e-6)
-    t0 = time.perf_counter()
-    for q in range(8):
-        g.seedset_ppr(sets[q], 300, 0.85, 1e-6)
-    out["plain_qps"] = 8 / (time.perf_counter() - t0)
+    # plain engine, one query at a time (reused pinned output buffer)
+    out["plain_qps"], _, _ = plain_engine_qps(g, sets, 16)
     for slots in slot_options:
         out[f"slots{slots}"] = _serve(pb, g, sets, rates, n_req, slots)
     g.close()
