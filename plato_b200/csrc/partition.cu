@@ -24,6 +24,20 @@
 // Padding rows have no edges; their state is held at the value an edgeless
 // vertex keeps, (1 - d) / V, so they add nothing to any delta and nothing
 // gathers them.
+//
+// Fused exchange (plato_partition_p2p_*), the B200 form of the same epoch:
+// every partition keeps two replicas of the whole state (ping-pong) and one
+// flag word per partition in its own HBM, and maps the other partitions'
+// replicas and flags (CUDA IPC between processes, plain pointers within
+// one).  The pull kernels store each new row value into all replicas at
+// once (peer stores over NVLink), so the exchange travels with the epoch's
+// own stores instead of following it; a one-thread kernel then publishes
+// the epoch (system-scope fence, release store of the epoch number into
+// this partition's flag on every GPU), and the next epoch starts with a
+// one-thread kernel that waits (acquire loads, bounded by a timeout) until
+// every partition has published.  Two replicas and a full barrier per epoch
+// mean no partition overwrites a replica another is still reading.  No
+// collective and no host round trip per epoch.
 #include <omp.h>
 #include <parallel/algorithm>
 
@@ -38,7 +52,25 @@ struct plato_partition {
   plato_graph* g = nullptr;  // this partition's rows (internal; never handed out)
   uint32_t rank = 0, world = 0, n = 0, real = 0, V = 0;
   std::vector<uint32_t> gid;  // caller id -> global internal id
-  ~plato_partition() { delete g; }
+  // fused exchange: local replicas and flags, the peers' mapped ones
+  float* s[2] = {nullptr, nullptr};
+  uint32_t* flags = nullptr;  // [world]: epochs published by each partition
+  int* status = nullptr;      // 1 once a wait gave up
+  float* peer_s[2][8] = {};
+  uint32_t* peer_flags[8] = {};
+  void* ipc_base[8][3] = {};  // mappings opened from IPC handles (closed on destroy)
+  bool p2p_ready = false;
+  uint64_t timeout_ns = 5000000000ull;
+  ~plato_partition() {
+    for (auto& peer : ipc_base)
+      for (void* b : peer)
+        if (b) cudaIpcCloseMemHandle(b);
+    for (float* b : s)
+      if (b) cudaFree(b);
+    if (flags) cudaFree(flags);
+    if (status) cudaFree(status);
+    delete g;
+  }
 };
 
 namespace plato_b200 {
@@ -47,6 +79,9 @@ namespace plato_b200 {
 int partition_prepare(plato_graph* g, cudaStream_t st);
 int pull_epoch_partition(plato_graph* g, const float* x_gather, const float* x_old, float* xn, float tele,
                          float d, bool final_epoch, cudaStream_t st, double* d_partial_sum);
+int pull_epoch_partition_bcast(plato_graph* g, const float* x_gather, const float* x_old, float* xn,
+                               float* const* peers, uint32_t npeers, float tele, float d, bool final_epoch,
+                               cudaStream_t st);
 
 namespace {
 
@@ -92,6 +127,62 @@ __global__ void k_part_init(const uint32_t* __restrict__ deg, uint32_t rows, uin
        v += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t dg = deg[v];
     x[v] = v >= real ? ghost : static_cast<float>(dg > 0 ? 1.0 / (static_cast<double>(V) * dg) : 1.0 / V);
+  }
+}
+
+// Peer pointers by value (kernel parameters): at most 8 partitions.
+struct peer_list {
+  float* p[8];
+};
+struct flag_list {
+  uint32_t* p[8];
+};
+
+// x0 of this partition's rows (as k_part_init) into every replica.
+__global__ void k_part_init_bcast(const uint32_t* __restrict__ deg, uint32_t rows, uint32_t real, uint32_t V,
+                                  float ghost, float* x, peer_list peers, uint32_t npeers) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < rows;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t dg = deg[v];
+    const float xv = v >= real ? ghost : static_cast<float>(dg > 0 ? 1.0 / (static_cast<double>(V) * dg) : 1.0 / V);
+    x[v] = xv;
+    for (uint32_t k = 0; k < npeers; ++k) peers.p[k][v] = xv;
+  }
+}
+
+// Publishes `value` as this partition's epoch count on every GPU: the
+// earlier kernels' stores (local and peer) are made visible at system scope
+// first, then each flag gets a release store.
+__global__ void k_p2p_signal(flag_list flags, uint32_t world, uint32_t rank, uint32_t value) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  __threadfence_system();
+  for (uint32_t q = 0; q < world; ++q)
+    asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(flags.p[q] + rank), "r"(value) : "memory");
+}
+
+// Waits until every partition has published at least `target` in the local
+// flags, for at most timeout_ns (the device's global timer); on a timeout it
+// sets *status and returns, and every later wait returns at once.
+__global__ void k_p2p_wait(const uint32_t* flags, uint32_t world, uint32_t target, int* status,
+                           uint64_t timeout_ns) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (*(volatile int*)status) return;
+  uint64_t t0;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  for (uint32_t q = 0; q < world; ++q) {
+    for (uint32_t spin = 0;; ++spin) {
+      uint32_t v;
+      asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(flags + q) : "memory");
+      if (v >= target) break;
+      uint64_t t;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+      if (t - t0 > timeout_ns || spin > (1u << 30)) {
+        *status = 1;
+        __threadfence_system();
+        return;
+      }
+      __nanosleep(256);
+    }
   }
 }
 
@@ -247,4 +338,167 @@ extern "C" int plato_partition_ranks(const plato_partition* p, const float* h_st
 #pragma omp parallel for schedule(static)
   for (int64_t v = 0; v < static_cast<int64_t>(p->V); ++v) ranks[v] = h_state[gid[v]];
   return PLATO_OK;
+}
+
+// ---- fused exchange over peer memory -----------------------------------------
+
+namespace {
+
+int p2p_alloc_local(plato_partition* p) {
+  if (p->world > 8) return set_error(PLATO_EINVAL, "partition p2p: at most 8 partitions");
+  PLATO_CUDA_TRY(cudaSetDevice(p->g->device));
+  if (p->s[0]) return PLATO_OK;
+  const size_t cells = static_cast<size_t>(p->world) * p->n;
+  for (float*& b : p->s) PLATO_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&b), cells * sizeof(float)));
+  PLATO_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&p->flags), p->world * sizeof(uint32_t)));
+  PLATO_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&p->status), sizeof(int)));
+  PLATO_CUDA_TRY(cudaMemset(p->flags, 0, p->world * sizeof(uint32_t)));
+  PLATO_CUDA_TRY(cudaMemset(p->status, 0, sizeof(int)));
+  for (int par = 0; par < 2; ++par) p->peer_s[par][p->rank] = p->s[par];
+  p->peer_flags[p->rank] = p->flags;
+  return PLATO_OK;
+}
+
+// The other partitions' slices of replica `par` at this partition's rows.
+plato_b200::peer_list p2p_peers(const plato_partition* p, int par) {
+  plato_b200::peer_list l{};
+  uint32_t k = 0;
+  const size_t base = static_cast<size_t>(p->rank) * p->n;
+  for (uint32_t q = 0; q < p->world; ++q)
+    if (q != p->rank) l.p[k++] = p->peer_s[par][q] + base;
+  return l;
+}
+
+plato_b200::flag_list p2p_flags(const plato_partition* p) {
+  plato_b200::flag_list l{};
+  for (uint32_t q = 0; q < p->world; ++q) l.p[q] = p->peer_flags[q];
+  return l;
+}
+
+}  // namespace
+
+extern "C" int plato_partition_p2p_alloc(plato_partition* p, void* handles) {
+  if (!p || !handles) return set_error(PLATO_EINVAL, "plato_partition_p2p_alloc: null argument");
+  PLATO_TRY(p2p_alloc_local(p));
+  auto* h = static_cast<cudaIpcMemHandle_t*>(handles);
+  PLATO_CUDA_TRY(cudaIpcGetMemHandle(h + 0, p->s[0]));
+  PLATO_CUDA_TRY(cudaIpcGetMemHandle(h + 1, p->s[1]));
+  PLATO_CUDA_TRY(cudaIpcGetMemHandle(h + 2, p->flags));
+  return PLATO_OK;
+}
+
+extern "C" int plato_partition_p2p_connect(plato_partition* p, const void* all_handles, uint32_t timeout_ms) {
+  if (!p || !all_handles) return set_error(PLATO_EINVAL, "plato_partition_p2p_connect: null argument");
+  if (!p->s[0]) return set_error(PLATO_EINVAL, "plato_partition_p2p_connect: call plato_partition_p2p_alloc first");
+  PLATO_CUDA_TRY(cudaSetDevice(p->g->device));
+  const auto* h = static_cast<const cudaIpcMemHandle_t*>(all_handles);
+  for (uint32_t q = 0; q < p->world; ++q) {
+    if (q == p->rank || p->ipc_base[q][0]) continue;
+    for (int i = 0; i < 3; ++i)
+      PLATO_CUDA_TRY(cudaIpcOpenMemHandle(&p->ipc_base[q][i], h[3 * q + i], cudaIpcMemLazyEnablePeerAccess));
+    p->peer_s[0][q] = static_cast<float*>(p->ipc_base[q][0]);
+    p->peer_s[1][q] = static_cast<float*>(p->ipc_base[q][1]);
+    p->peer_flags[q] = static_cast<uint32_t*>(p->ipc_base[q][2]);
+  }
+  p->timeout_ns = static_cast<uint64_t>(timeout_ms ? timeout_ms : 5000) * 1000000ull;
+  p->p2p_ready = true;
+  return PLATO_OK;
+}
+
+extern "C" int plato_partition_p2p_connect_local(plato_partition* const* parts, uint32_t world, uint32_t timeout_ms) {
+  if (!parts || world == 0 || world > 8) return set_error(PLATO_EINVAL, "plato_partition_p2p_connect_local: bad argument");
+  for (uint32_t r = 0; r < world; ++r) {
+    if (!parts[r] || parts[r]->world != world || parts[r]->rank != r)
+      return set_error(PLATO_EINVAL, "plato_partition_p2p_connect_local: parts[r] must be partition r of world");
+    PLATO_TRY(p2p_alloc_local(parts[r]));
+  }
+  for (uint32_t r = 0; r < world; ++r) {
+    plato_partition* p = parts[r];
+    for (uint32_t q = 0; q < world; ++q) {
+      const plato_partition* o = parts[q];
+      if (o->g->device != p->g->device) {  // partitions on several GPUs of one process
+        int ok = 0;
+        PLATO_CUDA_TRY(cudaDeviceCanAccessPeer(&ok, p->g->device, o->g->device));
+        if (!ok) return set_error(PLATO_EINVAL, "plato_partition_p2p_connect_local: no peer access between the GPUs");
+        PLATO_CUDA_TRY(cudaSetDevice(p->g->device));
+        const cudaError_t e = cudaDeviceEnablePeerAccess(o->g->device, 0);
+        if (e != cudaSuccess && e != cudaErrorPeerAccessAlreadyEnabled) PLATO_CUDA_TRY(e);
+        cudaGetLastError();
+      }
+      p->peer_s[0][q] = o->s[0];
+      p->peer_s[1][q] = o->s[1];
+      p->peer_flags[q] = o->flags;
+    }
+    p->timeout_ns = static_cast<uint64_t>(timeout_ms ? timeout_ms : 5000) * 1000000ull;
+    p->p2p_ready = true;
+  }
+  return PLATO_OK;
+}
+
+extern "C" int plato_partition_p2p_reset(plato_partition* p) {
+  if (!p || !p->s[0]) return set_error(PLATO_EINVAL, "plato_partition_p2p_reset: not allocated");
+  PLATO_CUDA_TRY(cudaSetDevice(p->g->device));
+  PLATO_CUDA_TRY(cudaMemset(p->flags, 0, p->world * sizeof(uint32_t)));
+  PLATO_CUDA_TRY(cudaMemset(p->status, 0, sizeof(int)));
+  return PLATO_OK;
+}
+
+extern "C" int plato_partition_p2p_init(plato_partition* p, double damping, void* stream) {
+  if (!p || !p->p2p_ready) return set_error(PLATO_EINVAL, "plato_partition_p2p_init: not connected");
+  if (!(damping >= 0.0 && damping <= 1.0)) return set_error(PLATO_EINVAL, "damping must be in [0, 1]");
+  PLATO_CUDA_TRY(cudaSetDevice(p->g->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const float ghost = static_cast<float>((1.0 - damping) / p->V);
+  k_part_init_bcast<<<grid_for(p->n, 256), 256, 0, st>>>(p->g->out_deg.p, p->n, p->real, p->V, ghost,
+                                                         p->s[0] + static_cast<size_t>(p->rank) * p->n,
+                                                         p2p_peers(p, 0), p->world - 1);
+  PLATO_LAUNCHED("k_part_init_bcast");
+  k_p2p_signal<<<1, 32, 0, st>>>(p2p_flags(p), p->world, p->rank, 1u);
+  PLATO_LAUNCHED("k_p2p_signal");
+  return PLATO_OK;
+}
+
+extern "C" int plato_partition_p2p_epoch(plato_partition* p, uint32_t epoch, double damping, int final_epoch,
+                                         void* stream) {
+  if (!p || !p->p2p_ready) return set_error(PLATO_EINVAL, "plato_partition_p2p_epoch: not connected");
+  if (!(damping >= 0.0 && damping <= 1.0)) return set_error(PLATO_EINVAL, "damping must be in [0, 1]");
+  if (epoch > 0xFFFFFFF0u) return set_error(PLATO_EINVAL, "plato_partition_p2p_epoch: epoch out of range");
+  PLATO_CUDA_TRY(cudaSetDevice(p->g->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int par = static_cast<int>(epoch & 1u);
+  // every partition has published epoch - 1 (init counts as 0): state[par] is complete here
+  k_p2p_wait<<<1, 32, 0, st>>>(p->flags, p->world, epoch + 1, p->status, p->timeout_ns);
+  PLATO_LAUNCHED("k_p2p_wait");
+  const size_t base = static_cast<size_t>(p->rank) * p->n;
+  const plato_b200::peer_list peers = p2p_peers(p, par ^ 1);
+  PLATO_TRY(pull_epoch_partition_bcast(p->g, p->s[par], p->s[par] + base, p->s[par ^ 1] + base, peers.p,
+                                       p->world - 1, static_cast<float>((1.0 - damping) / p->V),
+                                       static_cast<float>(damping), final_epoch != 0, st));
+  k_p2p_signal<<<1, 32, 0, st>>>(p2p_flags(p), p->world, p->rank, epoch + 2);
+  PLATO_LAUNCHED("k_p2p_signal");
+  return PLATO_OK;
+}
+
+extern "C" int plato_partition_p2p_state(plato_partition* p, uint32_t epochs, void* stream, const float** d_state) {
+  if (!p || !p->p2p_ready || !d_state) return set_error(PLATO_EINVAL, "plato_partition_p2p_state: bad argument");
+  PLATO_CUDA_TRY(cudaSetDevice(p->g->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  k_p2p_wait<<<1, 32, 0, st>>>(p->flags, p->world, epochs + 1, p->status, p->timeout_ns);
+  PLATO_LAUNCHED("k_p2p_wait");
+  int status = 0;
+  PLATO_CUDA_TRY(cudaMemcpyAsync(&status, p->status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  PLATO_CUDA_TRY(cudaStreamSynchronize(st));
+  if (status)
+    return set_error(PLATO_ETIMEDOUT, "partition p2p: a partition did not publish its epoch within the timeout");
+  *d_state = p->s[epochs & 1u];
+  return PLATO_OK;
+}
+
+extern "C" int plato_partition_p2p_ranks(plato_partition* p, uint32_t epochs, void* stream, float* ranks) {
+  if (!ranks) return set_error(PLATO_EINVAL, "plato_partition_p2p_ranks: null argument");
+  const float* d_state = nullptr;
+  PLATO_TRY(plato_partition_p2p_state(p, epochs, stream, &d_state));
+  std::vector<float> h(static_cast<size_t>(p->world) * p->n);
+  PLATO_CUDA_TRY(cudaMemcpy(h.data(), d_state, h.size() * sizeof(float), cudaMemcpyDeviceToHost));
+  return plato_partition_ranks(p, h.data(), ranks);
 }

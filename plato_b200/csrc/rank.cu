@@ -105,6 +105,39 @@ struct wrank_update {
   }
 };
 
+// PageRank update of one partition whose next state is replicated on every
+// partition's GPU: each new value is stored in the local replica and, over
+// peer memory (NVLink), at the same place in the other replicas, so the pull
+// epoch itself carries the exchange that an all-gather would do after it.
+constexpr uint32_t kMaxPartitionPeers = 7;  // 8 partitions (one node) at most
+struct bcast_rank_update {
+  rank_update<teleport_uniform> u;  // local replica: u.xn
+  float* peers[kMaxPartitionPeers];  // this partition's slice of the next state in the other replicas
+  uint32_t npeers;
+  using operands = rank_update<teleport_uniform>::operands;
+
+  __device__ __forceinline__ bool skip() const { return u.skip(); }
+  __device__ __forceinline__ operands load(uint32_t v) const { return u.load(v); }
+  __device__ __forceinline__ double apply(uint32_t v, float y) const { return apply(v, y, load(v)); }
+  __device__ __forceinline__ double apply(uint32_t v, float y, operands o) const {
+    const float r = fmaf(u.d, y, u.tele(v));
+    float xv = r;
+    double dl = 0.0;
+    if (!u.storing_rank()) {  // the update of rank_update::apply (pagerank.hpp:118-135)
+      if (o.dg > 0) {
+        const float fd = static_cast<float>(o.dg);
+        xv = r / fd;
+        dl = fabsf(xv - o.xo) * fd;
+      } else {
+        dl = fabsf(xv - o.xo);
+      }
+    }
+    u.xn[v] = xv;
+    for (uint32_t k = 0; k < npeers; ++k) peers[k][v] = xv;
+    return dl;
+  }
+};
+
 // Opts the kernel into the largest dynamic shared memory the device allows
 // next to its static shared memory; returns the hub capacity (floats) that fits.
 template <class Upd, bool kW = false>
@@ -240,6 +273,9 @@ int ensure_ws(plato_graph* g, cudaStream_t st) {
   uint32_t cap_c = 0, cap_d = 0;
   PLATO_TRY(set_pull_smem_attr<rank_update<teleport_seeds>>(g->device, &cap_c));
   PLATO_TRY((set_pull_smem_attr<wrank_update, true>(g->device, &cap_d)));
+  uint32_t cap_e = 0;
+  PLATO_TRY(set_pull_smem_attr<bcast_rank_update>(g->device, &cap_e));
+  cap_d = std::min(cap_d, cap_e);
   cap_b = std::min(cap_b, std::min(cap_c, cap_d));
   ws->hub_cap = std::min(cap_a, cap_b);
   return PLATO_OK;
@@ -683,6 +719,20 @@ int pull_epoch_partition(plato_graph* g, const float* x_gather, const float* x_o
     PLATO_LAUNCHED("k_sum_partials");
   }
   return PLATO_OK;
+}
+
+// The same epoch with the next state stored into every replica: xn is the
+// local slice, peers[k] the slices of the other replicas (peer memory).
+int pull_epoch_partition_bcast(plato_graph* g, const float* x_gather, const float* x_old, float* xn,
+                               float* const* peers, uint32_t npeers, float tele, float d, bool final_epoch,
+                               cudaStream_t st) {
+  if (npeers > kMaxPartitionPeers) return set_error(PLATO_EINVAL, "partition: more than 8 partitions");
+  PLATO_TRY(ensure_ws(g, st));
+  bcast_rank_update upd{};
+  upd.u = rank_update<teleport_uniform>{x_old, xn, g->out_deg.p, teleport_uniform{tele}, d, final_epoch ? 1 : 0};
+  for (uint32_t k = 0; k < npeers; ++k) upd.peers[k] = peers[k];
+  upd.npeers = npeers;
+  return pull_epoch_with<bcast_rank_update, false>(g, x_gather, upd, nullptr, st);
 }
 
 }  // namespace plato_b200

@@ -25,6 +25,8 @@ import numpy as np
 from . import _lib
 from ._lib import check, load
 
+IPC_HANDLE_BYTES = 64  # PLATO_IPC_HANDLE_BYTES
+
 
 def _u32(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.uint32)
@@ -80,6 +82,43 @@ class Partition:
                                                        1 if final else 0,
                                                        C.c_void_p(d_delta) if d_delta else None,
                                                        C.c_void_p(stream)), "plato_partition_pagerank_epoch")
+
+    # ---- fused exchange over peer memory (plato_partition_p2p_*) ----------------
+    def p2p_alloc(self) -> bytes:
+        """Allocates the two state replicas and the flags; -> their 3 CUDA IPC handles."""
+        h = C.create_string_buffer(3 * IPC_HANDLE_BYTES)
+        check(self._lib.plato_partition_p2p_alloc(self._h, h), "plato_partition_p2p_alloc")
+        return h.raw
+
+    def p2p_connect(self, all_handles: bytes, timeout_ms: int = 0):
+        """Maps the other partitions' replicas and flags (handles of every rank, rank order)."""
+        check(self._lib.plato_partition_p2p_connect(self._h, C.c_char_p(all_handles), timeout_ms),
+              "plato_partition_p2p_connect")
+
+    def p2p_reset(self):
+        check(self._lib.plato_partition_p2p_reset(self._h), "plato_partition_p2p_reset")
+
+    def p2p_init(self, damping: float, stream: int = 0):
+        check(self._lib.plato_partition_p2p_init(self._h, damping, C.c_void_p(stream)), "plato_partition_p2p_init")
+
+    def p2p_epoch(self, epoch: int, damping: float, final: bool, stream: int = 0):
+        check(self._lib.plato_partition_p2p_epoch(self._h, epoch, damping, 1 if final else 0, C.c_void_p(stream)),
+              "plato_partition_p2p_epoch")
+
+    def p2p_state(self, epochs: int, stream: int = 0) -> int:
+        """Waits for every partition's last epoch; -> device pointer of the
+        replica with the ranks (world * rows float32)."""
+        ptr = C.c_void_p()
+        check(self._lib.plato_partition_p2p_state(self._h, epochs, C.c_void_p(stream), C.byref(ptr)),
+              "plato_partition_p2p_state")
+        return int(ptr.value)
+
+    def p2p_ranks(self, epochs: int, stream: int = 0) -> np.ndarray:
+        """p2p_state, then the ranks in caller ids (float32 [V])."""
+        out = np.empty(self.vertices, np.float32)
+        check(self._lib.plato_partition_p2p_ranks(self._h, epochs, C.c_void_p(stream), C.c_void_p(out.ctypes.data)),
+              "plato_partition_p2p_ranks")
+        return out
 
     def ranks(self, h_state: np.ndarray) -> np.ndarray:
         """Caller-id ranks from the assembled state (host float32 [world * rows])."""
@@ -171,6 +210,59 @@ def emulate_partitions(vertices: int, src, dst, world: int, iterations: int = 10
 
         ran = _epochs(step, iterations, eps, delta_of)
         return parts[0].ranks(bufs[0].cpu().numpy()), ran
+    finally:
+        for p in parts:
+            p.close()
+
+
+def pagerank_partitioned_p2p(vertices: int, src, dst, iterations: int = 100, damping: float = 0.85,
+                             is_directed: bool = True, group=None, timeout_ms: int = 0):
+    """The partitioned PageRank with the fused exchange over peer memory: one
+    partition per process of `group` on its current GPU, CUDA IPC handles
+    exchanged once over torch.distributed, then `iterations` epochs with no
+    collective -> (caller-id ranks float32 [V], epochs)."""
+    import torch
+    import torch.distributed as dist
+
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    part = Partition(vertices, src, dst, rank, world, is_directed)
+    try:
+        handles = [None] * world
+        dist.all_gather_object(handles, part.p2p_alloc(), group=group)  # flags are zero before anyone maps them
+        part.p2p_connect(b"".join(handles), timeout_ms)
+        stream = torch.cuda.current_stream().cuda_stream
+        dist.barrier(group=group)  # every partition mapped and reset before any init publishes
+        part.p2p_init(damping, stream)
+        for e in range(iterations):
+            part.p2p_epoch(e, damping, e == iterations - 1, stream)
+        ranks = part.p2p_ranks(iterations, stream)
+        dist.barrier(group=group)  # no partition frees its replicas while a peer may still store into them
+        return ranks, iterations
+    finally:
+        part.close()
+
+
+def emulate_partitions_p2p(vertices: int, src, dst, world: int, iterations: int = 100, damping: float = 0.85,
+                           is_directed: bool = True, timeout_ms: int = 0):
+    """The fused exchange with `world` partitions in one process on the
+    current GPU: each epoch runs for every partition before the next epoch,
+    so every wait is already satisfied when it runs -> (caller-id ranks
+    float32 [V], epochs)."""
+    import torch
+
+    parts = [Partition(vertices, src, dst, r, world, is_directed) for r in range(world)]
+    try:
+        arr = (C.c_void_p * world)(*[p._h.value for p in parts])
+        check(load().plato_partition_p2p_connect_local(arr, world, timeout_ms), "plato_partition_p2p_connect_local")
+        stream = torch.cuda.current_stream().cuda_stream
+        for p in parts:
+            p.p2p_reset()
+        for p in parts:
+            p.p2p_init(damping, stream)
+        for e in range(iterations):
+            for p in parts:
+                p.p2p_epoch(e, damping, e == iterations - 1, stream)
+        return parts[0].p2p_ranks(iterations, stream), iterations
     finally:
         for p in parts:
             p.close()

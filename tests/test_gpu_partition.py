@@ -7,6 +7,13 @@
   RMAT graphs, with and without the eps exit.
 * The driver with its collectives over NCCL at world size 1 (the process
   group a torchrun job of one GPU has): same ranks.
+* The fused exchange over peer memory (plato_partition_p2p_*), P = 1..4
+  partitions in one process on one GPU, each epoch run for every partition
+  before the next (so every wait is already satisfied): the same ranks as
+  the all-gather path bit for bit, and plato_pagerank's within tolerance.
+* A wait that nothing satisfies (a partition that never publishes) gives up
+  after its timeout and the run reports PLATO_ETIMEDOUT; the GPU stays
+  usable.
 """
 import os
 import socket
@@ -66,3 +73,40 @@ def test_driver_over_nccl_world1():
         dist.destroy_process_group()
     assert ran == st.iterations
     assert float(np.abs(got.astype(np.float64) - want.astype(np.float64)).sum()) <= L1_TOL
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 4])
+@pytest.mark.parametrize("directed", [True, False])
+def test_p2p_exchange_equals_allgather_path(world, directed):
+    V, s, d = pb.rmat(15, 16, 17, symmetrize=not directed)
+    ref, ran_ref = partition.emulate_partitions(V, s, d, world, 30, 0.85, 0.0, directed)
+    got, ran = partition.emulate_partitions_p2p(V, s, d, world, 30, 0.85, directed)
+    assert ran == ran_ref == 30
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))  # the same row sums, bit for bit
+    with pb.Graph(V, s, d, directed) as g:
+        want, _ = g.pagerank(30, 0.85, 0.0)
+    assert float(np.abs(got.astype(np.float64) - want.astype(np.float64)).sum()) <= L1_TOL
+
+
+def test_p2p_wait_gives_up_and_reports_timeout():
+    import ctypes as C
+
+    from plato_b200 import _lib
+    V, s, d = pb.rmat(12, 16, 20)
+    parts = [partition.Partition(V, s, d, r, 2) for r in range(2)]
+    try:
+        arr = (C.c_void_p * 2)(*[p._h.value for p in parts])
+        _lib.check(_lib.load().plato_partition_p2p_connect_local(arr, 2, 200), "plato_partition_p2p_connect_local")
+        for p in parts:
+            p.p2p_reset()
+        parts[0].p2p_init(0.85)  # partition 1 never publishes its state
+        parts[0].p2p_epoch(0, 0.85, True)
+        with pytest.raises(pb.PlatoError) as e:
+            parts[0].p2p_state(1)
+        assert e.value.code == _lib.PLATO_ETIMEDOUT
+    finally:
+        for p in parts:
+            p.close()
+    with pb.Graph(V, s, d, True) as g:  # the context is still usable
+        r, st = g.pagerank(5)
+        assert st.iterations == 5 and np.isfinite(r).all()
