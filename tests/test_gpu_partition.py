@@ -110,3 +110,22 @@ def test_p2p_wait_gives_up_and_reports_timeout():
     with pb.Graph(V, s, d, True) as g:  # the context is still usable
         r, st = g.pagerank(5)
         assert st.iterations == 5 and np.isfinite(r).all()
+
+
+def test_p2p_driver_world1():
+    """pagerank_partitioned_p2p in a one-process group: its IPC handles are
+    made and exchanged, its epochs run with no collective."""
+    import datetime
+
+    import torch.distributed as dist
+    V, s, d = pb.rmat(14, 16, 21)
+    with pb.Graph(V, s, d, True) as g:
+        want, _ = g.pagerank(25, 0.85, 0.0)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(_free_port()))
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        got, ran = partition.pagerank_partitioned_p2p(V, s, d, 25, 0.85)
+    finally:
+        dist.destroy_process_group()
+    assert ran == 25
+    assert float(np.abs(got.astype(np.float64) - want.astype(np.float64)).sum()) <= L1_TOL
