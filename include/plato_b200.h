@@ -350,34 +350,38 @@ int plato_partition_ranks(const plato_partition* p, const float* h_state, float*
  * 88-144), with each partition's pull storing its new rows straight into the
  * state replicas of every partition (NVLink peer stores) and a flag per
  * partition published after each epoch; the next epoch starts once every
- * partition has published (a bounded wait on the device).  No collective and
- * no host round trip per epoch; at most 8 partitions; fixed-epoch runs (eps
- * 0; eps > 0 takes the all-gather path, whose delta is all-reduced).
+ * partition has published (a bounded wait on the device).  With eps > 0 each
+ * partition also publishes its delta, and every partition sums them in rank
+ * order and applies the eps exit of pagerank.hpp:137-139 on the device.  No
+ * collective and no host round trip per epoch; at most 8 partitions.
  * Between processes: every partition calls plato_partition_p2p_alloc
- * (two state replicas of world*rows floats and the flags, in its own HBM;
- * writes 3 CUDA IPC handles of PLATO_IPC_HANDLE_BYTES each), the handles of
- * all partitions are exchanged in rank order, then plato_partition_p2p_connect
- * maps the others'.  Partitions of one process (on one GPU, or on several
- * with peer access): plato_partition_p2p_connect_local.  A run: reset (flags
- * to 0 on every partition before any init), init on every partition, then
- * plato_partition_p2p_epoch for epoch 0 .. E-1 (final_epoch on the last), then
- * plato_partition_p2p_state(E), which waits for every partition's last epoch
- * and returns the replica that holds the ranks (world*rows floats, device;
- * map with plato_partition_ranks after copying it to the host).  A wait gives
- * up after timeout_ms (0: 5000) and the run reports PLATO_ETIMEDOUT from
- * plato_partition_p2p_state; later waits of the run return at once.  With
- * partitions of one process on one GPU, call each epoch for every partition
- * before the next epoch (each epoch's waits are then already satisfied). */
+ * (two state replicas of world*rows floats and a flag/delta block, in its
+ * own HBM; writes 3 CUDA IPC handles of PLATO_IPC_HANDLE_BYTES each), the
+ * handles of all partitions are exchanged in rank order, then
+ * plato_partition_p2p_connect maps the others'.  Partitions of one process
+ * (on one GPU, or on several with peer access): plato_partition_p2p_connect_local.
+ * A run: reset (flags to 0 on every partition, then a barrier, before any
+ * init; alloc leaves them 0), init on every partition, then
+ * plato_partition_p2p_epoch for epoch 0 .. iterations-1 (epochs after an eps
+ * exit only pass the barrier), then plato_partition_p2p_state, which waits
+ * for every partition's last epoch and returns the replica that holds the
+ * ranks (world*rows floats, device) and the epochs that ran; or
+ * plato_partition_p2p_ranks for the ranks in caller ids on the host.  A wait
+ * gives up after timeout_ms (0: 5000) and the run reports PLATO_ETIMEDOUT
+ * from plato_partition_p2p_state; later waits of the run return at once.
+ * With partitions of one process on one GPU, call each epoch for every
+ * partition before the next epoch (each epoch's waits are then already
+ * satisfied). */
 #define PLATO_IPC_HANDLE_BYTES 64
 int plato_partition_p2p_alloc(plato_partition* p, void* handles_out);
 int plato_partition_p2p_connect(plato_partition* p, const void* all_handles, uint32_t timeout_ms);
 int plato_partition_p2p_connect_local(plato_partition* const* parts, uint32_t world, uint32_t timeout_ms);
 int plato_partition_p2p_reset(plato_partition* p);
-int plato_partition_p2p_init(plato_partition* p, double damping, void* stream);
-int plato_partition_p2p_epoch(plato_partition* p, uint32_t epoch, double damping, int final_epoch, void* stream);
-int plato_partition_p2p_state(plato_partition* p, uint32_t epochs, void* stream, const float** d_state);
+int plato_partition_p2p_init(plato_partition* p, uint32_t iterations, double damping, double eps, void* stream);
+int plato_partition_p2p_epoch(plato_partition* p, uint32_t epoch, double damping, void* stream);
+int plato_partition_p2p_state(plato_partition* p, void* stream, const float** d_state, uint32_t* epochs);
 /* plato_partition_p2p_state, then the ranks in caller ids (host [V]). */
-int plato_partition_p2p_ranks(plato_partition* p, uint32_t epochs, void* stream, float* ranks);
+int plato_partition_p2p_ranks(plato_partition* p, void* stream, float* ranks, uint32_t* epochs);
 
 /* ---- diagnostics -----------------------------------------------------------
  * No counterpart in the reference.  The memory system's rate on this graph's

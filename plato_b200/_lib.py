@@ -140,10 +140,10 @@ SIGNATURES = {
     "plato_partition_p2p_connect": (C.c_int, [P, P, C.c_uint32]),
     "plato_partition_p2p_connect_local": (C.c_int, [P, C.c_uint32, C.c_uint32]),
     "plato_partition_p2p_reset": (C.c_int, [P]),
-    "plato_partition_p2p_init": (C.c_int, [P, C.c_double, P]),
-    "plato_partition_p2p_epoch": (C.c_int, [P, C.c_uint32, C.c_double, C.c_int, P]),
-    "plato_partition_p2p_state": (C.c_int, [P, C.c_uint32, P, C.POINTER(C.c_void_p)]),
-    "plato_partition_p2p_ranks": (C.c_int, [P, C.c_uint32, P, P]),
+    "plato_partition_p2p_init": (C.c_int, [P, C.c_uint32, C.c_double, C.c_double, P]),
+    "plato_partition_p2p_epoch": (C.c_int, [P, C.c_uint32, C.c_double, P]),
+    "plato_partition_p2p_state": (C.c_int, [P, P, C.POINTER(C.c_void_p), C.POINTER(C.c_uint32)]),
+    "plato_partition_p2p_ranks": (C.c_int, [P, P, P, C.POINTER(C.c_uint32)]),
     "plato_diag_pull_ceiling": (C.c_int, [P, C.c_uint32, C.c_uint32, C.POINTER(C.c_double),
                                           C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
     "plato_diag_batch_ceiling": (C.c_int, [P, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_double),

@@ -54,10 +54,18 @@ struct plato_partition {
   std::vector<uint32_t> gid;  // caller id -> global internal id
   // fused exchange: local replicas and flags, the peers' mapped ones
   float* s[2] = {nullptr, nullptr};
-  uint32_t* flags = nullptr;  // [world]: epochs published by each partition
-  int* status = nullptr;      // 1 once a wait gave up
+  // one synchronisation block per partition: [world] u32 epoch flags at byte
+  // 0, [2][world] double deltas at byte 64 (peers write both)
+  unsigned char* sync = nullptr;
+  uint32_t* flags = nullptr;
+  double* deltas = nullptr;
+  int* ctrl = nullptr;        // [4]: wait status (1 = gave up), epoch mode, epochs run, eps mode
+  double* d_part = nullptr;   // this partition's delta of the last epoch
   float* peer_s[2][8] = {};
   uint32_t* peer_flags[8] = {};
+  double* peer_deltas[8] = {};
+  double eps = 0.0;
+  uint32_t iterations = 0;
   void* ipc_base[8][3] = {};  // mappings opened from IPC handles (closed on destroy)
   bool p2p_ready = false;
   uint64_t timeout_ns = 5000000000ull;
@@ -67,8 +75,9 @@ struct plato_partition {
         if (b) cudaIpcCloseMemHandle(b);
     for (float* b : s)
       if (b) cudaFree(b);
-    if (flags) cudaFree(flags);
-    if (status) cudaFree(status);
+    if (sync) cudaFree(sync);
+    if (ctrl) cudaFree(ctrl);
+    if (d_part) cudaFree(d_part);
     delete g;
   }
 };
@@ -81,7 +90,7 @@ int pull_epoch_partition(plato_graph* g, const float* x_gather, const float* x_o
                          float d, bool final_epoch, cudaStream_t st, double* d_partial_sum);
 int pull_epoch_partition_bcast(plato_graph* g, const float* x_gather, const float* x_old, float* xn,
                                float* const* peers, uint32_t npeers, float tele, float d, bool final_epoch,
-                               cudaStream_t st);
+                               const int* mode, cudaStream_t st, double* d_partial_sum);
 
 namespace {
 
@@ -150,14 +159,53 @@ __global__ void k_part_init_bcast(const uint32_t* __restrict__ deg, uint32_t row
   }
 }
 
-// Publishes `value` as this partition's epoch count on every GPU: the
-// earlier kernels' stores (local and peer) are made visible at system scope
-// first, then each flag gets a release store.
-__global__ void k_p2p_signal(flag_list flags, uint32_t world, uint32_t rank, uint32_t value) {
+struct delta_list {
+  double* p[8];
+};
+
+// Publishes `value` as this partition's epoch count on every GPU: with
+// deltas, first this partition's delta of the epoch (*d_part) into slot
+// [slot][rank] of every GPU's deltas; then the earlier kernels' stores (local
+// and peer) are made visible at system scope, then each flag gets a release
+// store.
+__global__ void k_p2p_signal(flag_list flags, delta_list deltas, uint32_t world, uint32_t rank, uint32_t value,
+                             const double* d_part, uint32_t slot) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (d_part) {
+    const double dv = *d_part;
+    for (uint32_t q = 0; q < world; ++q) deltas.p[q][slot * world + rank] = dv;
+  }
   __threadfence_system();
   for (uint32_t q = 0; q < world; ++q)
     asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(flags.p[q] + rank), "r"(value) : "memory");
+}
+
+// The eps exit of pagerank.hpp:137-139 for the fused exchange, run by every
+// partition at the start of epoch `epoch` >= 1 once all have published epoch
+// - 1: the same rule as k_epoch_control on the delta summed over the
+// partitions in rank order (so every partition takes the same decision).
+// ctrl[1] = mode of this epoch (0 normal, 1 final, 2 done), ctrl[2] = epochs
+// run before it.
+__global__ void k_p2p_control(const double* deltas, uint32_t world, uint32_t epoch, int* ctrl, double scale,
+                              double eps, uint32_t iteration) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int mode = ctrl[1];
+  if (mode == 2) return;
+  const int ran = ctrl[2] + 1;
+  ctrl[2] = ran;
+  if (mode == 1) {
+    ctrl[1] = 2;
+    return;
+  }
+  const double* dv = deltas + ((epoch - 1) & 1u) * world;
+  double sum = 0.0;
+  for (uint32_t q = 0; q < world; ++q) {
+    double v;
+    asm volatile("ld.relaxed.sys.global.f64 %0, [%1];" : "=d"(v) : "l"(dv + q) : "memory");
+    sum += v;
+  }
+  const double dlt = sum * scale;
+  if ((eps > 0.0 && dlt < eps) || static_cast<uint32_t>(ran) >= iteration - 1) ctrl[1] = 1;
 }
 
 // Waits until every partition has published at least `target` in the local
@@ -344,18 +392,26 @@ extern "C" int plato_partition_ranks(const plato_partition* p, const float* h_st
 
 namespace {
 
+constexpr size_t kSyncDeltas = 64;  // byte offset of the deltas in the sync block
+
 int p2p_alloc_local(plato_partition* p) {
   if (p->world > 8) return set_error(PLATO_EINVAL, "partition p2p: at most 8 partitions");
   PLATO_CUDA_TRY(cudaSetDevice(p->g->device));
   if (p->s[0]) return PLATO_OK;
   const size_t cells = static_cast<size_t>(p->world) * p->n;
   for (float*& b : p->s) PLATO_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&b), cells * sizeof(float)));
-  PLATO_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&p->flags), p->world * sizeof(uint32_t)));
-  PLATO_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&p->status), sizeof(int)));
-  PLATO_CUDA_TRY(cudaMemset(p->flags, 0, p->world * sizeof(uint32_t)));
-  PLATO_CUDA_TRY(cudaMemset(p->status, 0, sizeof(int)));
+  const size_t sync_bytes = kSyncDeltas + 2ull * p->world * sizeof(double);
+  PLATO_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&p->sync), sync_bytes));
+  PLATO_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&p->ctrl), 4 * sizeof(int)));
+  PLATO_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&p->d_part), sizeof(double)));
+  PLATO_CUDA_TRY(cudaMemset(p->sync, 0, sync_bytes));
+  PLATO_CUDA_TRY(cudaMemset(p->ctrl, 0, 4 * sizeof(int)));
+  PLATO_CUDA_TRY(cudaMemset(p->d_part, 0, sizeof(double)));
+  p->flags = reinterpret_cast<uint32_t*>(p->sync);
+  p->deltas = reinterpret_cast<double*>(p->sync + kSyncDeltas);
   for (int par = 0; par < 2; ++par) p->peer_s[par][p->rank] = p->s[par];
   p->peer_flags[p->rank] = p->flags;
+  p->peer_deltas[p->rank] = p->deltas;
   return PLATO_OK;
 }
 
@@ -375,6 +431,12 @@ plato_b200::flag_list p2p_flags(const plato_partition* p) {
   return l;
 }
 
+plato_b200::delta_list p2p_deltas(const plato_partition* p) {
+  plato_b200::delta_list l{};
+  for (uint32_t q = 0; q < p->world; ++q) l.p[q] = p->peer_deltas[q];
+  return l;
+}
+
 }  // namespace
 
 extern "C" int plato_partition_p2p_alloc(plato_partition* p, void* handles) {
@@ -383,7 +445,7 @@ extern "C" int plato_partition_p2p_alloc(plato_partition* p, void* handles) {
   auto* h = static_cast<cudaIpcMemHandle_t*>(handles);
   PLATO_CUDA_TRY(cudaIpcGetMemHandle(h + 0, p->s[0]));
   PLATO_CUDA_TRY(cudaIpcGetMemHandle(h + 1, p->s[1]));
-  PLATO_CUDA_TRY(cudaIpcGetMemHandle(h + 2, p->flags));
+  PLATO_CUDA_TRY(cudaIpcGetMemHandle(h + 2, p->sync));
   return PLATO_OK;
 }
 
@@ -399,6 +461,7 @@ extern "C" int plato_partition_p2p_connect(plato_partition* p, const void* all_h
     p->peer_s[0][q] = static_cast<float*>(p->ipc_base[q][0]);
     p->peer_s[1][q] = static_cast<float*>(p->ipc_base[q][1]);
     p->peer_flags[q] = static_cast<uint32_t*>(p->ipc_base[q][2]);
+    p->peer_deltas[q] = reinterpret_cast<double*>(static_cast<unsigned char*>(p->ipc_base[q][2]) + kSyncDeltas);
   }
   p->timeout_ns = static_cast<uint64_t>(timeout_ms ? timeout_ms : 5000) * 1000000ull;
   p->p2p_ready = true;
@@ -428,6 +491,7 @@ extern "C" int plato_partition_p2p_connect_local(plato_partition* const* parts, 
       p->peer_s[0][q] = o->s[0];
       p->peer_s[1][q] = o->s[1];
       p->peer_flags[q] = o->flags;
+      p->peer_deltas[q] = o->deltas;
     }
     p->timeout_ns = static_cast<uint64_t>(timeout_ms ? timeout_ms : 5000) * 1000000ull;
     p->p2p_ready = true;
@@ -438,66 +502,87 @@ extern "C" int plato_partition_p2p_connect_local(plato_partition* const* parts, 
 extern "C" int plato_partition_p2p_reset(plato_partition* p) {
   if (!p || !p->s[0]) return set_error(PLATO_EINVAL, "plato_partition_p2p_reset: not allocated");
   PLATO_CUDA_TRY(cudaSetDevice(p->g->device));
-  PLATO_CUDA_TRY(cudaMemset(p->flags, 0, p->world * sizeof(uint32_t)));
-  PLATO_CUDA_TRY(cudaMemset(p->status, 0, sizeof(int)));
+  PLATO_CUDA_TRY(cudaMemset(p->sync, 0, kSyncDeltas + 2ull * p->world * sizeof(double)));
+  PLATO_CUDA_TRY(cudaMemset(p->ctrl, 0, 4 * sizeof(int)));
   return PLATO_OK;
 }
 
-extern "C" int plato_partition_p2p_init(plato_partition* p, double damping, void* stream) {
+extern "C" int plato_partition_p2p_init(plato_partition* p, uint32_t iterations, double damping, double eps,
+                                        void* stream) {
   if (!p || !p->p2p_ready) return set_error(PLATO_EINVAL, "plato_partition_p2p_init: not connected");
   if (!(damping >= 0.0 && damping <= 1.0)) return set_error(PLATO_EINVAL, "damping must be in [0, 1]");
+  if (iterations == 0 || iterations > 0x7FFFFFF0u) return set_error(PLATO_EINVAL, "iteration must be >= 1");
   PLATO_CUDA_TRY(cudaSetDevice(p->g->device));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  p->iterations = iterations;
+  p->eps = eps > 0.0 ? eps : 0.0;
+  // the device epoch control: mode of epoch 0, nothing run yet, eps mode
+  const int c[3] = {iterations == 1 ? 1 : 0, 0, p->eps > 0.0 ? 1 : 0};
+  PLATO_CUDA_TRY(cudaMemcpyAsync(p->ctrl + 1, c, sizeof(c), cudaMemcpyHostToDevice, st));
   const float ghost = static_cast<float>((1.0 - damping) / p->V);
   k_part_init_bcast<<<grid_for(p->n, 256), 256, 0, st>>>(p->g->out_deg.p, p->n, p->real, p->V, ghost,
                                                          p->s[0] + static_cast<size_t>(p->rank) * p->n,
                                                          p2p_peers(p, 0), p->world - 1);
   PLATO_LAUNCHED("k_part_init_bcast");
-  k_p2p_signal<<<1, 32, 0, st>>>(p2p_flags(p), p->world, p->rank, 1u);
+  k_p2p_signal<<<1, 32, 0, st>>>(p2p_flags(p), p2p_deltas(p), p->world, p->rank, 1u, nullptr, 0u);
   PLATO_LAUNCHED("k_p2p_signal");
   return PLATO_OK;
 }
 
-extern "C" int plato_partition_p2p_epoch(plato_partition* p, uint32_t epoch, double damping, int final_epoch,
-                                         void* stream) {
-  if (!p || !p->p2p_ready) return set_error(PLATO_EINVAL, "plato_partition_p2p_epoch: not connected");
+extern "C" int plato_partition_p2p_epoch(plato_partition* p, uint32_t epoch, double damping, void* stream) {
+  if (!p || !p->p2p_ready || p->iterations == 0)
+    return set_error(PLATO_EINVAL, "plato_partition_p2p_epoch: not initialised");
+  if (epoch >= p->iterations) return set_error(PLATO_EINVAL, "plato_partition_p2p_epoch: epoch >= iterations");
   if (!(damping >= 0.0 && damping <= 1.0)) return set_error(PLATO_EINVAL, "damping must be in [0, 1]");
-  if (epoch > 0xFFFFFFF0u) return set_error(PLATO_EINVAL, "plato_partition_p2p_epoch: epoch out of range");
   PLATO_CUDA_TRY(cudaSetDevice(p->g->device));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int par = static_cast<int>(epoch & 1u);
-  // every partition has published epoch - 1 (init counts as 0): state[par] is complete here
-  k_p2p_wait<<<1, 32, 0, st>>>(p->flags, p->world, epoch + 1, p->status, p->timeout_ns);
+  const bool eps_mode = p->eps > 0.0;
+  // every partition has published epoch - 1 (init counts as 0): state[par],
+  // and with eps their deltas of epoch - 1, are complete here
+  k_p2p_wait<<<1, 32, 0, st>>>(p->flags, p->world, epoch + 1, p->ctrl, p->timeout_ns);
   PLATO_LAUNCHED("k_p2p_wait");
+  if (eps_mode && epoch > 0) {
+    k_p2p_control<<<1, 32, 0, st>>>(p->deltas, p->world, epoch, p->ctrl, static_cast<double>(p->V), p->eps,
+                                    p->iterations);
+    PLATO_LAUNCHED("k_p2p_control");
+  }
   const size_t base = static_cast<size_t>(p->rank) * p->n;
   const plato_b200::peer_list peers = p2p_peers(p, par ^ 1);
   PLATO_TRY(pull_epoch_partition_bcast(p->g, p->s[par], p->s[par] + base, p->s[par ^ 1] + base, peers.p,
                                        p->world - 1, static_cast<float>((1.0 - damping) / p->V),
-                                       static_cast<float>(damping), final_epoch != 0, st));
-  k_p2p_signal<<<1, 32, 0, st>>>(p2p_flags(p), p->world, p->rank, epoch + 2);
+                                       static_cast<float>(damping), epoch + 1 == p->iterations,
+                                       eps_mode ? p->ctrl + 1 : nullptr, st, eps_mode ? p->d_part : nullptr));
+  k_p2p_signal<<<1, 32, 0, st>>>(p2p_flags(p), p2p_deltas(p), p->world, p->rank, epoch + 2,
+                                 eps_mode ? p->d_part : nullptr, epoch & 1u);
   PLATO_LAUNCHED("k_p2p_signal");
   return PLATO_OK;
 }
 
-extern "C" int plato_partition_p2p_state(plato_partition* p, uint32_t epochs, void* stream, const float** d_state) {
-  if (!p || !p->p2p_ready || !d_state) return set_error(PLATO_EINVAL, "plato_partition_p2p_state: bad argument");
+extern "C" int plato_partition_p2p_state(plato_partition* p, void* stream, const float** d_state, uint32_t* epochs) {
+  if (!p || !p->p2p_ready || p->iterations == 0 || !d_state)
+    return set_error(PLATO_EINVAL, "plato_partition_p2p_state: bad argument");
   PLATO_CUDA_TRY(cudaSetDevice(p->g->device));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  k_p2p_wait<<<1, 32, 0, st>>>(p->flags, p->world, epochs + 1, p->status, p->timeout_ns);
+  k_p2p_wait<<<1, 32, 0, st>>>(p->flags, p->world, p->iterations + 1, p->ctrl, p->timeout_ns);
   PLATO_LAUNCHED("k_p2p_wait");
-  int status = 0;
-  PLATO_CUDA_TRY(cudaMemcpyAsync(&status, p->status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  int c[3] = {0, 0, 0};
+  PLATO_CUDA_TRY(cudaMemcpyAsync(c, p->ctrl, sizeof(c), cudaMemcpyDeviceToHost, st));
   PLATO_CUDA_TRY(cudaStreamSynchronize(st));
-  if (status)
+  if (c[0])
     return set_error(PLATO_ETIMEDOUT, "partition p2p: a partition did not publish its epoch within the timeout");
-  *d_state = p->s[epochs & 1u];
+  // fixed epochs: all ran; with eps: those counted by the control, plus a
+  // final epoch that no later control counted
+  const uint32_t ran = p->eps > 0.0 ? static_cast<uint32_t>(c[2]) + (c[1] == 1 ? 1u : 0u) : p->iterations;
+  if (epochs) *epochs = ran;
+  *d_state = p->s[ran & 1u];
   return PLATO_OK;
 }
 
-extern "C" int plato_partition_p2p_ranks(plato_partition* p, uint32_t epochs, void* stream, float* ranks) {
+extern "C" int plato_partition_p2p_ranks(plato_partition* p, void* stream, float* ranks, uint32_t* epochs) {
   if (!ranks) return set_error(PLATO_EINVAL, "plato_partition_p2p_ranks: null argument");
   const float* d_state = nullptr;
-  PLATO_TRY(plato_partition_p2p_state(p, epochs, stream, &d_state));
+  PLATO_TRY(plato_partition_p2p_state(p, stream, &d_state, epochs));
   std::vector<float> h(static_cast<size_t>(p->world) * p->n);
   PLATO_CUDA_TRY(cudaMemcpy(h.data(), d_state, h.size() * sizeof(float), cudaMemcpyDeviceToHost));
   return plato_partition_ranks(p, h.data(), ranks);

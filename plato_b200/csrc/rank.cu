@@ -723,16 +723,26 @@ int pull_epoch_partition(plato_graph* g, const float* x_gather, const float* x_o
 
 // The same epoch with the next state stored into every replica: xn is the
 // local slice, peers[k] the slices of the other replicas (peer memory).
+// `mode` (device, or null): the epoch kind decided on the device (0 normal,
+// 1 final, 2 done, as k_epoch_control); d_partial_sum (or null) receives the
+// epoch's delta partials summed (normalised units).
 int pull_epoch_partition_bcast(plato_graph* g, const float* x_gather, const float* x_old, float* xn,
                                float* const* peers, uint32_t npeers, float tele, float d, bool final_epoch,
-                               cudaStream_t st) {
+                               const int* mode, cudaStream_t st, double* d_partial_sum) {
   if (npeers > kMaxPartitionPeers) return set_error(PLATO_EINVAL, "partition: more than 8 partitions");
   PLATO_TRY(ensure_ws(g, st));
   bcast_rank_update upd{};
-  upd.u = rank_update<teleport_uniform>{x_old, xn, g->out_deg.p, teleport_uniform{tele}, d, final_epoch ? 1 : 0};
+  upd.u = rank_update<teleport_uniform>{x_old, xn, g->out_deg.p, teleport_uniform{tele}, d, final_epoch ? 1 : 0,
+                                        mode};
   for (uint32_t k = 0; k < npeers; ++k) upd.peers[k] = peers[k];
   upd.npeers = npeers;
-  return pull_epoch_with<bcast_rank_update, false>(g, x_gather, upd, nullptr, st);
+  PLATO_TRY((pull_epoch_with<bcast_rank_update, false>(g, x_gather, upd, nullptr, st)));
+  if (d_partial_sum) {
+    k_sum_partials<<<1, 1024, 0, st>>>(g->rank_ws->partials.p, static_cast<uint32_t>(partial_count(g)),
+                                       d_partial_sum);
+    PLATO_LAUNCHED("k_sum_partials");
+  }
+  return PLATO_OK;
 }
 
 }  // namespace plato_b200

@@ -98,27 +98,29 @@ class Partition:
     def p2p_reset(self):
         check(self._lib.plato_partition_p2p_reset(self._h), "plato_partition_p2p_reset")
 
-    def p2p_init(self, damping: float, stream: int = 0):
-        check(self._lib.plato_partition_p2p_init(self._h, damping, C.c_void_p(stream)), "plato_partition_p2p_init")
+    def p2p_init(self, iterations: int, damping: float, eps: float = 0.0, stream: int = 0):
+        check(self._lib.plato_partition_p2p_init(self._h, iterations, damping, eps, C.c_void_p(stream)),
+              "plato_partition_p2p_init")
 
-    def p2p_epoch(self, epoch: int, damping: float, final: bool, stream: int = 0):
-        check(self._lib.plato_partition_p2p_epoch(self._h, epoch, damping, 1 if final else 0, C.c_void_p(stream)),
+    def p2p_epoch(self, epoch: int, damping: float, stream: int = 0):
+        check(self._lib.plato_partition_p2p_epoch(self._h, epoch, damping, C.c_void_p(stream)),
               "plato_partition_p2p_epoch")
 
-    def p2p_state(self, epochs: int, stream: int = 0) -> int:
-        """Waits for every partition's last epoch; -> device pointer of the
-        replica with the ranks (world * rows float32)."""
-        ptr = C.c_void_p()
-        check(self._lib.plato_partition_p2p_state(self._h, epochs, C.c_void_p(stream), C.byref(ptr)),
+    def p2p_state(self, stream: int = 0):
+        """Waits for every partition's last epoch; -> (device pointer of the
+        replica with the ranks (world * rows float32), epochs run)."""
+        ptr, ep = C.c_void_p(), C.c_uint32()
+        check(self._lib.plato_partition_p2p_state(self._h, C.c_void_p(stream), C.byref(ptr), C.byref(ep)),
               "plato_partition_p2p_state")
-        return int(ptr.value)
+        return int(ptr.value), int(ep.value)
 
-    def p2p_ranks(self, epochs: int, stream: int = 0) -> np.ndarray:
-        """p2p_state, then the ranks in caller ids (float32 [V])."""
+    def p2p_ranks(self, stream: int = 0):
+        """p2p_state, then -> (ranks in caller ids float32 [V], epochs run)."""
         out = np.empty(self.vertices, np.float32)
-        check(self._lib.plato_partition_p2p_ranks(self._h, epochs, C.c_void_p(stream), C.c_void_p(out.ctypes.data)),
-              "plato_partition_p2p_ranks")
-        return out
+        ep = C.c_uint32()
+        check(self._lib.plato_partition_p2p_ranks(self._h, C.c_void_p(stream), C.c_void_p(out.ctypes.data),
+                                                  C.byref(ep)), "plato_partition_p2p_ranks")
+        return out, int(ep.value)
 
     def ranks(self, h_state: np.ndarray) -> np.ndarray:
         """Caller-id ranks from the assembled state (host float32 [world * rows])."""
@@ -216,11 +218,12 @@ def emulate_partitions(vertices: int, src, dst, world: int, iterations: int = 10
 
 
 def pagerank_partitioned_p2p(vertices: int, src, dst, iterations: int = 100, damping: float = 0.85,
-                             is_directed: bool = True, group=None, timeout_ms: int = 0):
+                             eps: float = 0.0, is_directed: bool = True, group=None, timeout_ms: int = 0):
     """The partitioned PageRank with the fused exchange over peer memory: one
     partition per process of `group` on its current GPU, CUDA IPC handles
-    exchanged once over torch.distributed, then `iterations` epochs with no
-    collective -> (caller-id ranks float32 [V], epochs)."""
+    exchanged once over torch.distributed, then the epochs with no collective
+    (the eps exit, if any, decided on every GPU from the published deltas)
+    -> (caller-id ranks float32 [V], epochs)."""
     import torch
     import torch.distributed as dist
 
@@ -231,19 +234,19 @@ def pagerank_partitioned_p2p(vertices: int, src, dst, iterations: int = 100, dam
         dist.all_gather_object(handles, part.p2p_alloc(), group=group)  # flags are zero before anyone maps them
         part.p2p_connect(b"".join(handles), timeout_ms)
         stream = torch.cuda.current_stream().cuda_stream
-        dist.barrier(group=group)  # every partition mapped and reset before any init publishes
-        part.p2p_init(damping, stream)
+        dist.barrier(group=group)  # every partition mapped before any init publishes
+        part.p2p_init(iterations, damping, eps, stream)
         for e in range(iterations):
-            part.p2p_epoch(e, damping, e == iterations - 1, stream)
-        ranks = part.p2p_ranks(iterations, stream)
+            part.p2p_epoch(e, damping, stream)
+        ranks, ran = part.p2p_ranks(stream)
         dist.barrier(group=group)  # no partition frees its replicas while a peer may still store into them
-        return ranks, iterations
+        return ranks, ran
     finally:
         part.close()
 
 
 def emulate_partitions_p2p(vertices: int, src, dst, world: int, iterations: int = 100, damping: float = 0.85,
-                           is_directed: bool = True, timeout_ms: int = 0):
+                           eps: float = 0.0, is_directed: bool = True, timeout_ms: int = 0):
     """The fused exchange with `world` partitions in one process on the
     current GPU: each epoch runs for every partition before the next epoch,
     so every wait is already satisfied when it runs -> (caller-id ranks
@@ -258,11 +261,11 @@ def emulate_partitions_p2p(vertices: int, src, dst, world: int, iterations: int 
         for p in parts:
             p.p2p_reset()
         for p in parts:
-            p.p2p_init(damping, stream)
+            p.p2p_init(iterations, damping, eps, stream)
         for e in range(iterations):
             for p in parts:
-                p.p2p_epoch(e, damping, e == iterations - 1, stream)
-        return parts[0].p2p_ranks(iterations, stream), iterations
+                p.p2p_epoch(e, damping, stream)
+        return parts[0].p2p_ranks(stream)
     finally:
         for p in parts:
             p.close()

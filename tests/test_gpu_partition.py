@@ -76,15 +76,18 @@ def test_driver_over_nccl_world1():
 
 
 @pytest.mark.parametrize("world", [1, 2, 3, 4])
-@pytest.mark.parametrize("directed", [True, False])
-def test_p2p_exchange_equals_allgather_path(world, directed):
+@pytest.mark.parametrize("directed,eps", [(True, 0.0), (False, 0.0), (True, 0.001)])
+def test_p2p_exchange_equals_allgather_path(world, directed, eps):
     V, s, d = pb.rmat(15, 16, 17, symmetrize=not directed)
-    ref, ran_ref = partition.emulate_partitions(V, s, d, world, 30, 0.85, 0.0, directed)
-    got, ran = partition.emulate_partitions_p2p(V, s, d, world, 30, 0.85, directed)
-    assert ran == ran_ref == 30
+    ref, ran_ref = partition.emulate_partitions(V, s, d, world, 30, 0.85, eps, directed)
+    got, ran = partition.emulate_partitions_p2p(V, s, d, world, 30, 0.85, eps, directed)
+    assert ran == ran_ref
+    if eps == 0.0:
+        assert ran == 30
     assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))  # the same row sums, bit for bit
     with pb.Graph(V, s, d, directed) as g:
-        want, _ = g.pagerank(30, 0.85, 0.0)
+        want, st = g.pagerank(30, 0.85, eps)
+    assert ran == st.iterations
     assert float(np.abs(got.astype(np.float64) - want.astype(np.float64)).sum()) <= L1_TOL
 
 
@@ -99,10 +102,10 @@ def test_p2p_wait_gives_up_and_reports_timeout():
         _lib.check(_lib.load().plato_partition_p2p_connect_local(arr, 2, 200), "plato_partition_p2p_connect_local")
         for p in parts:
             p.p2p_reset()
-        parts[0].p2p_init(0.85)  # partition 1 never publishes its state
-        parts[0].p2p_epoch(0, 0.85, True)
+        parts[0].p2p_init(1, 0.85)  # partition 1 never publishes its state
+        parts[0].p2p_epoch(0, 0.85)
         with pytest.raises(pb.PlatoError) as e:
-            parts[0].p2p_state(1)
+            parts[0].p2p_state()
         assert e.value.code == _lib.PLATO_ETIMEDOUT
     finally:
         for p in parts:
@@ -119,13 +122,13 @@ def test_p2p_driver_world1():
 
     import torch.distributed as dist
     V, s, d = pb.rmat(14, 16, 21)
-    with pb.Graph(V, s, d, True) as g:
-        want, _ = g.pagerank(25, 0.85, 0.0)
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(_free_port()))
     dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
     try:
-        got, ran = partition.pagerank_partitioned_p2p(V, s, d, 25, 0.85)
+        got, ran = partition.pagerank_partitioned_p2p(V, s, d, 25, 0.85, 0.001)
     finally:
         dist.destroy_process_group()
-    assert ran == 25
+    with pb.Graph(V, s, d, True) as g:
+        want, st = g.pagerank(25, 0.85, 0.001)
+    assert ran == st.iterations
     assert float(np.abs(got.astype(np.float64) - want.astype(np.float64)).sum()) <= L1_TOL
