@@ -27,7 +27,12 @@ namespace plato_b200 {
 
 enum : uint8_t { COL_FREE = 0, COL_LIVE = 1, COL_FINAL = 2, COL_DONE = 3 };
 
-constexpr int kBatchTile = 2048;  // merge items per CTA (1024: 5-9% slower at RMAT s22-s24)
+// Merge items per CTA by column-tile width.  2048 below kt 128; 3072 at kt
+// 128, where a group's row pieces are wider (one B200, queries/s against
+// 2048: RMAT s22 K = 256 / 1024 +0.2% / +1.1%, RMAT s24 K = 128 +1.3%; at
+// kt 64 RMAT s22 K = 64 -1.2%).  1024 was 5-9% slower; 4096 (41 KB of shared
+// memory) leaves fewer CTAs per SM and loses 10%.
+constexpr int batch_tile_items(int kt) { return kt >= 128 ? 3072 : 2048; }
 // Row gathers in flight per lane and CTAs per SM of k_batch_pull: 4 at 5 CTAs
 // beat 8 at 4 (K = 64: 103.6 -> 100.9 ms per batch at RMAT s22; 6 or 8 at 5
 // CTAs spill and lose 7%).
@@ -213,7 +218,7 @@ __device__ __forceinline__ void merge_search(const uint32_t* s_rowend, int nrows
 
 template <int GL, int VEC>
 __global__ void __launch_bounds__(256, kBatchMinBlocks) k_batch_pull(batch_pass p0) {
-  constexpr int KT = GL * VEC, NG = 256 / GL, TILE = kBatchTile, IPG = TILE / NG;
+  constexpr int KT = GL * VEC, NG = 256 / GL, TILE = batch_tile_items(KT), IPG = TILE / NG;
   const batch_pass p = batch_tile_view<KT>(p0);
   // The row ends and staged source ids are dead once the gathers are done, so
   // the per-lane delta partials reuse their space; the head row's sums wait in

@@ -147,7 +147,7 @@ int batch_engine::init(uint32_t K, uint32_t kt, uint32_t max_iterations, double 
     hot_l2_bytes_ = static_cast<uint64_t>(l2) / 2;
   }
   const merge_tiles* mt = nullptr;
-  PLATO_TRY(ensure_pull_tiles(g_, kBatchTile, st_, &mt));
+  PLATO_TRY(ensure_pull_tiles(g_, batch_tile_items(static_cast<int>(kt)), st_, &mt));
   const uint32_t T = mt->count;
   const uint32_t NG = 256 / group_lanes(kt);
   rows_ = T + (T + NG - 1) / NG;
@@ -190,7 +190,7 @@ int batch_engine::init(uint32_t K, uint32_t kt, uint32_t max_iterations, double 
 
 int batch_engine::launch_iteration(int parity) {
   const uint32_t V = g_->info.vertices;
-  const merge_tiles& mt = g_->tiles.at(kBatchTile);
+  const merge_tiles& mt = g_->tiles.at(batch_tile_items(static_cast<int>(kt_)));
   batch_pass p{};
   p.trow = mt.row.p;
   p.tedge = mt.edge.p;
