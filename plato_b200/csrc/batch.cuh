@@ -98,15 +98,18 @@ __device__ __forceinline__ void ldvec(const float* p, float (&a)[VEC]) {
   }
 }
 
-// 16-byte load with an L2 cache policy (createpolicy).  The row gathers of
-// the hottest rows (the first hot_rows vertices: on a relabelled graph the
-// highest in-degrees, which on these graphs are also the most gathered) are
-// plain loads; all colder rows are loaded evict-first, so they do not push
-// the hot rows out of L2.  hot_rows covers half of L2 for one column tile
-// (tiles run one after another).  Measured on one B200 against plain loads
-// for every row (queries/s, RMAT s24 K = 64 / 128 / 256, RMAT s22 K = 64 /
-// 256 / 1024): +6% / +8% / +8%, +2% / +6% / +6%; 3/4 of L2 or all of it
-// gain a little less, and marking the hot rows evict-last gained nothing.
+// 16-byte load with an L2 cache policy (createpolicy).  k_batch_pull gathers
+// every row through one range policy: the hottest rows (the first hot_rows
+// vertices: on a relabelled graph the highest in-degrees, which on these
+// graphs are also the most gathered; half of L2 for one column tile, as the
+// tiles of a launch run one after another) at normal priority, all colder
+// rows evict-first, so they do not push the hot rows out of L2.  Against
+// plain loads for every row the split gained 2-8%; making it by address (one
+// load form, no compare per gather) instead of choosing between a plain and
+// an evict-first load per row gained another 4-14% (one B200, queries/s,
+// RMAT s22 K = 64 / 256 / 1024: 630 / 753 / 773 -> 716 / 792 / 818; RMAT
+// s24 K = 64 / 128: 158.5 / 173 -> 171 / 179).  Choosing between two policy
+// registers per gather gains nothing.
 __device__ __forceinline__ void ld4_pol(const float* p, float (&a)[4], uint64_t pol) {
   asm("ld.global.nc.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
       : "=f"(a[0]), "=f"(a[1]), "=f"(a[2]), "=f"(a[3])
@@ -233,8 +236,19 @@ __global__ void __launch_bounds__(256, kBatchMinBlocks) k_batch_pull(batch_pass 
   __shared__ uint32_t s_ckey[NG];
   __shared__ float s_cval[NG * KT];
   __shared__ float s_hacc[NG * KT];
-  uint64_t pol_cold;  // L2 evict-first, for the gathers of rows past hot_rows
-  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol_cold));
+  // One L2 policy for every row gather, by address: normal priority for the
+  // hot rows [0, hot_rows) of this column tile, evict-first past them (range
+  // sizes are 32-bit: rows past 4 GB of a tile keep the default priority).
+  uint64_t pol;
+  {
+    const uint64_t tile_bytes = static_cast<uint64_t>(p.V) * KT * 4;
+    const uint32_t total = static_cast<uint32_t>(tile_bytes < 0xFFFFFF00ull ? tile_bytes : 0xFFFFFF00ull);
+    const uint64_t hot_bytes = static_cast<uint64_t>(p.hot_rows) * KT * 4;
+    const uint32_t primary = static_cast<uint32_t>(hot_bytes < total ? hot_bytes : total);
+    asm("createpolicy.range.global.L2::evict_normal.L2::evict_first.b64 %0, [%1], %2, %3;"
+        : "=l"(pol)
+        : "l"(p.X), "r"(primary), "r"(total));
+  }
 
   const int lane_g = threadIdx.x % GL, g = threadIdx.x / GL;
   uint8_t st[VEC];
@@ -295,10 +309,7 @@ __global__ void __launch_bounds__(256, kBatchMinBlocks) k_batch_pull(batch_pass 
         if (u < n) {
           const uint32_t src = s_src[jj + u];
           static_assert(VEC == 4, "row gathers are 16-byte loads");
-          if (src < p.hot_rows)
-            ldvec<VEC>(xl + static_cast<size_t>(src) * KT, a[u]);
-          else
-            ld4_pol(xl + static_cast<size_t>(src) * KT, a[u], pol_cold);
+          ld4_pol(xl + static_cast<size_t>(src) * KT, a[u], pol);
         } else {
 #pragma unroll
           for (int c = 0; c < VEC; ++c) a[u][c] = 0.f;
