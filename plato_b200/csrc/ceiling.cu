@@ -85,8 +85,9 @@ __global__ void __launch_bounds__(256, (M <= 8 ? 8 : 4)) k_ceil_gather(const uin
 
 // Batched-pull row gathers: a group of GL lanes takes 4 consecutive edges of
 // the whole CSC id stream at a time and gathers the source's kt-float row
-// (kt = 4 GL, a float4 per lane, 4 rows in flight per lane, rows at or past
-// keep_rows loaded evict-first in L2, as k_batch_pull).
+// (kt = 4 GL, a float4 per lane, 4 rows in flight per lane, every row
+// through one L2 range policy: rows below keep_rows at normal priority, the
+// rest evict-first, as k_batch_pull).
 // kMode: 0 the edge's own source row, 1 row = edge position mod V (sequential
 // rows: the streaming rate of the same instruction mix), 2 source folded into
 // the first hot_rows rows (an L2-resident block).
@@ -96,9 +97,16 @@ __global__ void __launch_bounds__(256, 5) k_ceil_rows(const uint32_t* __restrict
                                                       uint32_t hot_rows, uint32_t keep_rows,
                                                       float* __restrict__ sink) {
   constexpr int KT = GL * 4;
-  uint64_t pol_keep, pol_cold;
-  asm("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(pol_keep));
-  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol_cold));
+  uint64_t pol;
+  {
+    const uint64_t bytes = static_cast<uint64_t>(V) * KT * 4;
+    const uint32_t total = static_cast<uint32_t>(bytes < 0xFFFFFF00ull ? bytes : 0xFFFFFF00ull);
+    const uint64_t keep = static_cast<uint64_t>(keep_rows) * KT * 4;
+    const uint32_t primary = static_cast<uint32_t>(keep < total ? keep : total);
+    asm("createpolicy.range.global.L2::evict_normal.L2::evict_first.b64 %0, [%1], %2, %3;"
+        : "=l"(pol)
+        : "l"(X), "r"(primary), "r"(total));
+  }
   const unsigned lane_g = threadIdx.x % GL;
   const uint64_t groups = (uint64_t)gridDim.x * (blockDim.x / GL);
   float s = 0.f;
@@ -120,7 +128,7 @@ __global__ void __launch_bounds__(256, 5) k_ceil_rows(const uint32_t* __restrict
       if (e0 + u < n)
         asm("ld.global.nc.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
             : "=f"(a[u].x), "=f"(a[u].y), "=f"(a[u].z), "=f"(a[u].w)
-            : "l"(X + static_cast<size_t>(row[u]) * KT + 4 * lane_g), "l"(row[u] < keep_rows ? pol_keep : pol_cold));
+            : "l"(X + static_cast<size_t>(row[u]) * KT + 4 * lane_g), "l"(pol));
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) s += (a[u].x + a[u].y) + (a[u].z + a[u].w);
