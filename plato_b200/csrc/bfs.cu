@@ -14,7 +14,10 @@
 // One kernel launch per level (k_bfs_level): it runs the push or the pull
 // step that the previous level chose, clears the frontier buffer that the
 // level after next fills, and its last CTA to finish counts the new frontier
-// and chooses the next level's mode (no CTA waits for another).
+// and chooses the next level's mode (no CTA waits for another).  A search's
+// start (root in, state cleared, root seeded, first mode chosen), its first
+// 8 levels and the read of the control word are one CUDA graph per graph and
+// threshold, so the host issues one launch where it issued 16 calls.
 #include <algorithm>
 #include <new>
 
@@ -41,8 +44,16 @@ struct bfs_workspace {
   dbuf<bfs_control> ctrl;
   bfs_control* h_ctrl = nullptr;  // pinned
   unsigned level_blocks = 0;      // one full wave of resident k_bfs_level CTAs
+  dbuf<uint32_t> root;            // the search's root (internal id) on the device
+  uint32_t* h_root = nullptr;     // pinned; copied to `root` by the start graph
+  // start graph (see bfs_impl) and what it was captured with
+  cudaGraphExec_t start = nullptr;
+  double start_threshold = -1.0;
+  const void* start_key = nullptr;
   ~bfs_workspace() {
+    if (start) cudaGraphExecDestroy(start);
     if (h_ctrl) cudaFreeHost(h_ctrl);
+    if (h_root) cudaFreeHost(h_root);
   }
 };
 
@@ -50,8 +61,9 @@ void destroy_bfs_workspace(bfs_workspace* ws) { delete ws; }
 
 namespace {
 
-__global__ void k_bfs_init(uint32_t V, uint32_t root, uint32_t invalid_parent, uint32_t* level,
-                           uint32_t* parent, uint32_t* visited) {
+__global__ void k_bfs_init(uint32_t V, const uint32_t* __restrict__ root_p, uint32_t invalid_parent,
+                           uint32_t* level, uint32_t* parent, uint32_t* visited) {
+  const uint32_t root = *root_p;
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
        v += (uint64_t)gridDim.x * blockDim.x) {
     level[v] = v == root ? 0u : PLATO_LEVEL_UNREACHED;
@@ -79,14 +91,6 @@ struct bfs_level_args {
   bfs_control* ctrl;
   double edges, threshold;
 };
-
-__device__ __forceinline__ void bfs_visit(const bfs_level_args& a, uint32_t v, uint32_t par) {
-  a.level[v] = a.new_level;
-  a.parent[v] = par;
-  const uint32_t bit = 1u << (v & 31);
-  atomicOr(&a.visited[v >> 5], bit);
-  atomicOr(&a.next.bits[v >> 5], bit);
-}
 
 // Claims dst for parent u if nobody has (bfs.hpp:97-118: CAS on the parent);
 // `word` is a recent read of dst's visited word (bits are only ever set, and
@@ -334,8 +338,11 @@ int ensure_bfs_ws(plato_graph* g) {
   PLATO_TRY(ws->level.alloc(V));
   PLATO_TRY(ws->parent.alloc(V));
   PLATO_TRY(ws->ctrl.alloc(1));
+  PLATO_TRY(ws->root.alloc(1));
   if (!ws->h_ctrl)
     PLATO_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&ws->h_ctrl), sizeof(bfs_control)));
+  if (!ws->h_root)
+    PLATO_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&ws->h_root), sizeof(uint32_t)));
   return PLATO_OK;
 }
 
@@ -359,6 +366,58 @@ __global__ void k_bfs_start(bfs_control* c, const unsigned long long* counters, 
   *c = bfs_control{push ? 1 : 0, 0, 0, 0, 1ull, push ? 1ull : 0ull, 0u};
 }
 
+constexpr uint32_t kFirstBatch = 8;  // RMAT searches end within about 8 levels
+constexpr uint64_t kStartKernels = 3 + kFirstBatch;  // init, seed, start, levels
+
+// k_frontier_seed for a root held on the device (the start graph's copy).
+__global__ void k_frontier_seed_at(frontier_view f, const uint32_t* __restrict__ vp,
+                                   const uint32_t* __restrict__ deg) {
+  // one warp
+  const uint32_t v = *vp;
+  const bool take = (threadIdx.x == 0);
+  if (take) atomicOr(&f.bits[v >> 5], 1u << (v & 31));
+  frontier_append_warp(f, take, v, deg);
+}
+
+// A launch inside a capture: its error is checked, and it is counted once
+// per replay of the graph instead of at capture.
+#define BFS_CAPTURED(name)                                                                  \
+  do {                                                                                      \
+    cudaError_t bfs_e_ = cudaGetLastError();                                                \
+    if (bfs_e_ != cudaSuccess)                                                              \
+      return set_error(PLATO_ECUDA, std::string("launch of ") + (name) + " failed: " +     \
+                                        cudaGetErrorString(bfs_e_));                       \
+  } while (0)
+
+// The start graph's work (captured by bfs_impl): the root copied in from
+// pinned memory, level / parent / visited cleared with the root set, the
+// frontiers reset and seeded with the root, the first level's mode
+// (bfs.hpp:86-96), kFirstBatch levels and the control word copied out.
+int enqueue_start(plato_graph* g, bfs_workspace* ws, bfs_level_args a, uint32_t invalid_parent,
+                  cudaStream_t st) {
+  const uint32_t V = g->info.vertices;
+  PLATO_CUDA_TRY(cudaMemcpyAsync(ws->root.p, ws->h_root, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  k_bfs_init<<<grid_for(V, 256), 256, 0, st>>>(V, ws->root.p, invalid_parent, ws->level.p, ws->parent.p,
+                                                ws->visited.p);
+  BFS_CAPTURED("k_bfs_init");
+  PLATO_TRY(frontier_reset(ws->fr[0], V, st));
+  PLATO_TRY(frontier_reset(ws->fr[1], V, st));
+  k_frontier_seed_at<<<1, 32, 0, st>>>(ws->fr[0].view(), ws->root.p, g->out_deg.p);
+  BFS_CAPTURED("k_frontier_seed_at");
+  k_bfs_start<<<1, 1, 0, st>>>(ws->ctrl.p, ws->fr[0].counters.p, a.edges, a.threshold);
+  BFS_CAPTURED("k_bfs_start");
+  for (uint32_t launched = 0; launched < kFirstBatch; ++launched) {
+    a.cur = ws->fr[launched % 3].view();
+    a.next = ws->fr[(launched + 1) % 3].view();
+    a.spare = ws->fr[(launched + 2) % 3].view();
+    a.new_level = launched + 1;
+    k_bfs_level<<<ws->level_blocks, 256, 0, st>>>(a);
+    BFS_CAPTURED("k_bfs_level");
+  }
+  PLATO_CUDA_TRY(cudaMemcpyAsync(ws->h_ctrl, ws->ctrl.p, sizeof(bfs_control), cudaMemcpyDeviceToHost, st));
+  return PLATO_OK;
+}
+
 int bfs_impl(plato_graph* g, const plato_bfs_opts* o, const plato_dualmode_opts* eo,
              cudaStream_t st, plato_run_stats* stats) {
   const uint32_t V = g->info.vertices;
@@ -370,27 +429,13 @@ int bfs_impl(plato_graph* g, const plato_bfs_opts* o, const plato_dualmode_opts*
   PLATO_TRY(host_to_internal(g, &to_int, st));
   const uint32_t root = to_int ? (*to_int)[o->root] : o->root;
   const uint32_t invalid_parent = g->info.max_v_i + 1;  // bfs.hpp:79
-  k_bfs_init<<<grid_for(V, 256), 256, 0, st>>>(V, root, invalid_parent, ws->level.p, ws->parent.p,
-                                                ws->visited.p);
-  PLATO_LAUNCHED("k_bfs_init");
-  PLATO_TRY(frontier_reset(ws->fr[0], V, st));
-  PLATO_TRY(frontier_reset(ws->fr[1], V, st));
-  PLATO_TRY(frontier_seed(ws->fr[0], g, root, st));
-
-  // Level loop with the engine switch on the device (k_bfs_level).  The host
-  // enqueues levels in batches and polls between batches; levels enqueued
-  // after the end return at once.  Nothing is read back before the first
-  // poll: the first level's mode is set on the device too.
   const double edges = static_cast<double>(g->stored_edges);
-  k_bfs_start<<<1, 1, 0, st>>>(ws->ctrl.p, ws->fr[0].counters.p, edges, threshold);
-  PLATO_LAUNCHED("k_bfs_start");
   if (ws->level_blocks == 0) {  // one full wave of resident CTAs; the steps stride over their work
     int sms = 0, per_sm = 0;
     PLATO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
     PLATO_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bfs_level, 256, 0));
     ws->level_blocks = static_cast<unsigned>(sms) * static_cast<unsigned>(std::max(per_sm, 1));
   }
-  const unsigned blocks = ws->level_blocks;
   bfs_level_args a{};
   a.V = V;
   a.out_off = g->out_off.p;
@@ -404,21 +449,50 @@ int bfs_impl(plato_graph* g, const plato_bfs_opts* o, const plato_dualmode_opts*
   a.ctrl = ws->ctrl.p;
   a.edges = edges;
   a.threshold = threshold;
-  uint32_t launched = 0;
-  uint32_t batch = 8;  // RMAT searches end within about 8 levels
-  for (;;) {
-    for (uint32_t k = 0; k < batch; ++k, ++launched) {
+  // The start graph: root in, state cleared, root seeded, first mode (decided
+  // on the device from the seeded frontier's degree sum), the first
+  // kFirstBatch levels and the control word out.  Levels enqueued after the
+  // end return at once.  Captured once per graph and threshold; the buffers
+  // it names never move (grow-only, sized by V), and the key below catches it
+  // if they ever do.
+  const void* key = ws->level.p;
+  if (!ws->start || ws->start_threshold != threshold || ws->start_key != key) {
+    if (ws->start) cudaGraphExecDestroy(ws->start);
+    ws->start = nullptr;
+    cudaGraph_t graph = nullptr;
+    PLATO_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const int rc = enqueue_start(g, ws, a, invalid_parent, st);
+    const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+    if (rc != PLATO_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (ec != cudaSuccess) return set_error(PLATO_ECUDA, std::string("bfs: capture failed: ") + cudaGetErrorString(ec));
+    const cudaError_t ei = cudaGraphInstantiate(&ws->start, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {
+      ws->start = nullptr;
+      return set_error(PLATO_ECUDA, std::string("bfs: graph instantiation failed: ") + cudaGetErrorString(ei));
+    }
+    ws->start_threshold = threshold;
+    ws->start_key = key;
+  }
+  *ws->h_root = root;  // read by the graph's first node
+  PLATO_CUDA_TRY(cudaGraphLaunch(ws->start, st));
+  count_launch(kStartKernels);
+  PLATO_CUDA_TRY(cudaStreamSynchronize(st));
+  // Rare deeper searches: more levels in batches, one poll each.
+  for (uint32_t launched = kFirstBatch; !ws->h_ctrl->done;) {
+    for (uint32_t k = 0; k < 4; ++k, ++launched) {
       a.cur = ws->fr[launched % 3].view();
       a.next = ws->fr[(launched + 1) % 3].view();
       a.spare = ws->fr[(launched + 2) % 3].view();
       a.new_level = launched + 1;
-      k_bfs_level<<<blocks, 256, 0, st>>>(a);
+      k_bfs_level<<<ws->level_blocks, 256, 0, st>>>(a);
       PLATO_LAUNCHED("k_bfs_level");
     }
     PLATO_CUDA_TRY(cudaMemcpyAsync(ws->h_ctrl, ws->ctrl.p, sizeof(bfs_control), cudaMemcpyDeviceToHost, st));
     PLATO_CUDA_TRY(cudaStreamSynchronize(st));
-    if (ws->h_ctrl->done) break;
-    batch = 4;
   }
   const bfs_control& c = *ws->h_ctrl;
   if (stats) {
