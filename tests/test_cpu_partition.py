@@ -9,6 +9,10 @@
   restatement of the partition pull, test infrastructure standing in for the
   GPU kernel), all-gathers the next state in place and all-reduces the delta
   for the eps exit; the ranks equal the oracle's single-graph PageRank.
+* The fused-exchange driver (pagerank_partitioned_p2p) at world size 2 over
+  gloo, with a stand-in for the partition: every rank receives the IPC
+  handles of all ranks in rank order and drives its partition through
+  connect, init, the epochs, the ranks and close, on the current stream.
 """
 import os
 import socket
@@ -124,3 +128,67 @@ def test_partition_protocol_gloo_world2_matches_oracle(eps):
         ranks, ran = res[rank]
         assert ran == ep
         assert np.abs(np.asarray(ranks) - want / V).sum() <= 1e-12
+
+
+def _p2p_driver_worker(rank, world, port, out):
+    """pagerank_partitioned_p2p's host side at world size 2 over gloo, with a
+    stand-in for the partition (the library calls need a GPU): what each rank
+    sends and receives, and in which order it drives its partition."""
+    import datetime
+    import types
+
+    import torch
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    calls = []
+
+    class StandIn:
+        def __init__(self, vertices, src, dst, r, w, is_directed=True):
+            calls.append(("new", r, w, is_directed))
+            self.r = r
+
+        def p2p_alloc(self):
+            return bytes([self.r + 1]) * (3 * partition.IPC_HANDLE_BYTES)
+
+        def p2p_connect(self, all_handles, timeout_ms=0):
+            calls.append(("connect", all_handles, timeout_ms))
+
+        def p2p_init(self, iterations, damping, eps=0.0, stream=0):
+            calls.append(("init", iterations, damping, eps, stream))
+
+        def p2p_epoch(self, epoch, damping, stream=0):
+            calls.append(("epoch", epoch, stream))
+
+        def p2p_ranks(self, stream=0):
+            calls.append(("ranks", stream))
+            return np.full(4, self.r, np.float32), 3
+
+        def close(self):
+            calls.append(("close",))
+
+    partition.Partition = StandIn
+    torch.cuda.current_stream = lambda: types.SimpleNamespace(cuda_stream=77)
+    s = np.array([0, 1, 2], np.uint32)
+    d = np.array([1, 2, 3], np.uint32)
+    ranks, ran = partition.pagerank_partitioned_p2p(4, s, d, 5, 0.85, 0.001, False, None, 250)
+    out[rank] = (calls, ranks.tolist(), ran)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_p2p_driver_gloo_world2_exchanges_handles_in_rank_order():
+    port = _free_port()
+    with mp.get_context("spawn").Manager() as mgr:
+        out = mgr.dict()
+        mp.start_processes(_p2p_driver_worker, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
+        res = dict(out)
+    hb = 3 * partition.IPC_HANDLE_BYTES
+    handles = b"\x01" * hb + b"\x02" * hb
+    for rank in (0, 1):
+        calls, ranks, ran = res[rank]
+        assert calls[0] == ("new", rank, 2, False)
+        assert calls[1] == ("connect", handles, 250)
+        assert calls[2] == ("init", 5, 0.85, 0.001, 77)
+        assert calls[3:8] == [("epoch", e, 77) for e in range(5)]
+        assert calls[8:] == [("ranks", 77), ("close",)]
+        assert ranks == [float(rank)] * 4 and ran == 3
